@@ -1,0 +1,472 @@
+"""Benchmark of the RBF-FD assembly hot path on B200.
+
+Workload (one step = one pass of the hot path over one node set): the
+periodic 1024 x 1024 jittered grid (1,048,576 nodes, seed 2), k = 35 nearest
+neighbours (periodic k-NN), PHS r^5 + degree-3 polynomials (n = 45), three
+operators (Laplacian, d/dx, d/dy), FP32 factorisation with FP64 iterative
+refinement (the mixed form), FP64 weights written as CSR values. Every step
+runs the k-NN search and the assembly; inputs (16 MB of nodes) are resident
+in HBM, the 147 MB stencil table and 881 MB of weights are rewritten each
+step, so every step moves more than the 126 MB L2.
+
+Also reported on the same node set: the plain FP64 kernel (the denominator
+of the mixed/FP64 ratio), the max relative weight error of both against the
+FP64 CPU oracle on a stencil sample, the end-to-end rate through the host-
+buffer entry point (pinned host memory, copies inside the timed region), a
+bounded serving run, and the CPU baseline.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun (N > 1) every rank assembles its own node set (weak scaling,
+no data-path collective); rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "gpu-assembly_b200"))
+sys.path.insert(0, str(ROOT / "oracle"))
+
+M_GRID = 1024
+K, P, Q = 35, 3, 5
+NRHS = 3
+N_SYS = K + (P + 1) * (P + 2) // 2  # 45
+FLOP_PER_STENCIL = 2.0 / 3.0 * N_SYS ** 3 + 2 * NRHS * N_SYS ** 2  # 72,900
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return json.loads(p.read_text()), "measured"
+        except Exception:
+            pass
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+class Clocks:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [v.strip() for v in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_baseline_sample(seconds_cap=30.0):
+    """The CPU path on a bounded sample: the reference's ckdtree periodic
+    search (oracle/_ref, when built) + the oracle's FP64 assembly, OpenMP on
+    all host threads, on a 256 x 256 periodic jittered grid (65,536
+    stencils, same k, degree and jitter as the workload: the per-stencil
+    cost does not depend on the node count)."""
+    import oracle as O
+    from rbf_b200 import nodesets as NS
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    x, y, _ = NS.jittered_grid(256, 0.3, seed=2, periodic=True)
+    n = x.size
+    t0 = time.perf_counter()
+    if O.ref() is not None:
+        ja = O.ref_kdtree_stencils(x, y, K, period=(1.0, 1.0))
+        kind_knn = "reference ckdtree (KdTree::knn_stencils)"
+    else:
+        ja = O.knn_brute(x, y, K, period=(1.0, 1.0))
+        kind_knn = "oracle brute force"
+    t1 = time.perf_counter()
+    O.assemble(x, y, ja, K, P, period=(1.0, 1.0))
+    t2 = time.perf_counter()
+    return {"value": n / (t2 - t0), "unit": "stencils/s", "cores": cores, "kind": "port",
+            "sample": f"periodic 256x256 jittered grid ({n} stencils), k={K}, P={P}: {kind_knn} "
+                      f"{t1 - t0:.3f} s + oracle FP64 assembly (CPU restatement, OpenMP) "
+                      f"{t2 - t1:.3f} s"}
+
+
+def reference_arm(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    import oracle as O
+    from rbf_b200 import nodesets as NS
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    x, y, _ = NS.jittered_grid(256, 0.3, seed=2, periodic=True)
+    n = x.size
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        ja = (O.ref_kdtree_stencils(x, y, K, period=(1.0, 1.0)) if O.ref() is not None
+              else O.knn_brute(x, y, K, period=(1.0, 1.0)))
+        O.assemble(x, y, ja, K, P, period=(1.0, 1.0))
+        if i >= args.warmup:
+            times.append(time.perf_counter() - t0)
+    T = sum(times)
+    v = n * len(times) / T
+    line = {"metric": "stencils/s k=35 deg3 (periodic 1024^2 jittered grid, 3 operators)",
+            "value": v, "unit": "stencils/s", "impl": "reference", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * T / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded jittered grid)",
+            "config": {"workload": "periodic 256x256 sample of the 1024x1024 jittered grid, k=35, "
+                                   "r^5 + degree 3, Laplacian/dx/dy, FP64",
+                       "stencils_per_step": n},
+            "cpu_baseline": {"value": v, "unit": "stencils/s", "cores": cores,
+                             "kind": "reference" if O.ref() is not None else "port",
+                             "sample": "k-NN: the reference's own ckdtree search compiled from its "
+                                       "sources; assembly: the oracle's CPU restatement (the "
+                                       "reference has no CPU assembly)"},
+            "e2e": {"value": v, "unit": "stencils/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def traffic_per_launch():
+    """DRAM bytes per launch of the dominant kernel, from the committed ncu
+    summary (profiles/), scaled to the full workload; None if absent."""
+    p = ROOT / "profiles" / "asm_mixed_periodic1024.txt"
+    if not p.exists():
+        return None
+    for ln in p.read_text().splitlines():
+        if ln.startswith("traffic_bytes_per_launch_full:"):
+            try:
+                return float(ln.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--grid", type=int, default=M_GRID)
+    ap.add_argument("--serve-requests", type=int, default=200)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import torch
+    import oracle as O
+    import rbf_b200 as R
+    from rbf_b200 import nodesets as NS
+
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    m = args.grid
+    x, y, _ = NS.jittered_grid(m, 0.3, seed=2 + 1000 * rank, periodic=True)
+    n = x.size
+    nk = n * K
+    dev = torch.device("cuda", local)
+    xd = torch.as_tensor(x, device=dev)
+    yd = torch.as_tensor(y, device=dev)
+    ja = torch.empty(nk, dtype=torch.int32, device=dev)
+    vals = [torch.empty(nk, dtype=torch.float64, device=dev) for _ in range(NRHS)]
+    info = torch.empty(n, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    per = (1.0, 1.0)
+    ctx = R.Context(local)
+    d_mix = R.make_desc(P, Q, R.DEFAULT_OPS, R.FP32_IR, True, period=per)
+    d_f64 = R.make_desc(P, Q, R.DEFAULT_OPS, R.FP64, True, period=per)
+
+    def step(desc, stats=False):
+        ctx.knn_stencils(xd, yd, K, ja, period=per, stream=stream)
+        return ctx.assemble(desc, xd, yd, K, ja, vals, info, stats=stats, stream=stream)
+
+    def timed(desc, steps, warmup):
+        for _ in range(warmup):
+            step(desc)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        l0 = ctx.launches()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            step(desc)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1) / steps
+        return max_over_ranks(ms), ctx.launches() - l0
+
+    # ---- correctness of this run against the FP64 oracle on a sample
+    st_mix = step(d_mix, stats=True)
+    torch.cuda.synchronize()
+    ja_h = ja.cpu().numpy()
+    rows = np.random.default_rng(1).choice(n, 2048, replace=False)
+    idx = (rows[:, None] * K + np.arange(K)[None, :]).ravel()
+    W_mix = np.stack([v.cpu().numpy()[idx] for v in vals])
+    step(d_f64)
+    torch.cuda.synchronize()
+    W_64 = np.stack([v.cpu().numpy()[idx] for v in vals])
+    # FP64 oracle on the sampled stencils: renumber the nodes so the sampled
+    # centres come first, then assemble just those rows
+    O.set_threads(os.cpu_count() or 1)
+    order = np.concatenate([rows, np.setdiff1d(np.arange(n), rows)])
+    inv = np.empty(n, np.int64)
+    inv[order] = np.arange(n)
+    ja_s = inv[ja_h.reshape(n, K)[rows]].astype(np.int32).ravel()
+    ia_s = (np.arange(rows.size + 1) * K).astype(np.int32)
+    Wo, _ = O.assemble_csr(x[order], y[order], ia_s, ja_s, P=P, Q=Q, period=per,
+                           nstencils=rows.size)
+    err_mix = float(O.max_rel_err(W_mix, Wo, K).max())
+    err_64 = float(O.max_rel_err(W_64, Wo, K).max())
+
+    # ---- timed: mixed (headline) and FP64 on the same node set
+    with Clocks(local) as clk:
+        ms_mix, launches = timed(d_mix, args.steps, args.warmup)
+    ms_64, _ = timed(d_f64, max(3, args.steps // 2), args.warmup)
+    # dominant kernel alone: the assembly (k-NN excluded), CUDA events on its stream
+    step(d_mix)
+    torch.cuda.synchronize()
+    ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 5
+    ea.record(stream)
+    for _ in range(reps):
+        ctx.assemble(d_mix, xd, yd, K, ja, vals, info, stream=stream)
+    eb.record(stream)
+    torch.cuda.synchronize()
+    ms_asm = ea.elapsed_time(eb) / reps
+    ea.record(stream)
+    for _ in range(reps):
+        ctx.knn_stencils(xd, yd, K, ja, period=per, stream=stream)
+    eb.record(stream)
+    torch.cuda.synchronize()
+    ms_knn = ea.elapsed_time(eb) / reps
+    ea.record(stream)
+    for _ in range(reps):
+        ctx.assemble(d_f64, xd, yd, K, ja, vals, info, stream=stream)
+    eb.record(stream)
+    torch.cuda.synchronize()
+    ms_asm64 = ea.elapsed_time(eb) / reps
+
+    # ---- end to end through the host-buffer entry point (pinned host memory)
+    xh = torch.from_numpy(x).pin_memory()
+    yh = torch.from_numpy(y).pin_memory()
+    vh = [torch.empty(nk, dtype=torch.float64).pin_memory() for _ in range(NRHS)]
+    jh = torch.empty(nk, dtype=torch.int32).pin_memory()
+    e2e_steps = max(3, args.steps // 2)
+    for _ in range(2):
+        ctx.assemble_host(d_mix, xh, yh, K, vh, ja_out_h=jh)
+    barrier()
+    t0 = time.perf_counter()
+    e2e_dev_ms = 0.0
+    for _ in range(e2e_steps):
+        st = ctx.assemble_host(d_mix, xh, yh, K, vh, ja_out_h=jh)
+        e2e_dev_ms += st["ms"]
+    t1 = time.perf_counter()
+    barrier()
+    e2e_ms = max_over_ranks(1e3 * (t1 - t0) / e2e_steps)
+
+    # ---- serving sample (rank 0 only)
+    serving = None
+    if rank == 0 and not args.no_serve and args.serve_requests > 0:
+        serving = serve_sample(R, NS, local, args.serve_requests)
+
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return 0
+    pk, src = peaks()
+    flops = FLOP_PER_STENCIL * n
+    achieved = flops / (ms_asm * 1e-3) / 1e12
+    fp32_peak, fp32_src = fp32_peak_tflops()
+    line = {
+        "metric": "stencils/s k=35 deg3 (periodic 1024^2 jittered grid, 3 operators)",
+        "value": ws * n / (ms_mix * 1e-3),
+        "unit": "stencils/s",
+        "n_gpus": ws,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_mix,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32+f64",
+        "data": "synthetic (seeded jittered grid, numpy default_rng)",
+        "config": {"workload": f"periodic {m}x{m} jittered grid (+-0.3h), k={K} k-NN + "
+                               f"assembly, PHS r^{Q} + degree {P} (n={N_SYS}), Laplacian/dx/dy, "
+                               "FP32 LU + FP64 refinement",
+                   "stencils_per_gpu": n, "l2": "inputs and outputs > L2 every step",
+                   "precision": "FP32 factorisation + FP64 residual refinement, FP64 fallback"},
+        "fp64": {"stencils_per_s": ws * n / (ms_64 * 1e-3), "ms_per_step": ms_64,
+                 "asm_ms": ms_asm64},
+        "mixed_over_fp64": ms_64 / ms_mix,
+        "max_rel_weight_err": {"mixed": err_mix, "fp64": err_64,
+                               "vs": "FP64 CPU oracle, 2048 sampled stencils"},
+        "fallback_stencils": st_mix["fallback"] if st_mix else None,
+        "sweeps_mean": (st_mix["sweeps"] / max(1, n)) if st_mix else None,
+        "stages_ms": {"knn": ms_knn, "assembly_mixed": ms_asm, "assembly_fp64": ms_asm64},
+        "e2e": {"value": ws * n / (e2e_ms * 1e-3), "unit": "stencils/s",
+                "h2d_bytes_per_step": 16 * n,
+                "d2h_bytes_per_step": nk * (8 * NRHS + 4),
+                "device_ms": e2e_dev_ms / e2e_steps},
+        "gpu_launches": launches,
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+                     "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                     "traffic": traffic_per_launch(),
+                     "peak_source": fp32_src,
+                     "flop_per_stencil": FLOP_PER_STENCIL,
+                     "hbm": {"algorithmic_bytes": n * (44 * K + 16),
+                             "achieved_gbs": n * (44 * K + 16) / (ms_asm * 1e-3) / 1e9,
+                             "peak_gbs": pk.get("hbm_gbs"), "peak_source": src}},
+        "clocks": clk.summary(),
+    }
+    if serving is not None:
+        line["serving"] = serving
+    if not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline_sample()
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def fp32_peak_tflops():
+    """FP32 FMA peak of this GPU: 2 flops x 128 lanes x SMs x max SM clock
+    (the CUDA-core rate the assembly kernel is bound by)."""
+    import torch
+    props = torch.cuda.get_device_properties(torch.cuda.current_device())
+    pk, _ = peaks()
+    mhz = pk.get("sm_max_mhz") or 1965.0
+    return 2 * 128 * props.multi_processor_count * mhz * 1e6 / 1e12, \
+        f"nominal: 2 x 128 FP32 lanes x {props.multi_processor_count} SMs x {mhz:.0f} MHz"
+
+
+def serve_sample(R, NS, device, count):
+    """A bounded serving run: `count` requests of the serving mix (sizes
+    log-uniform in [1e3, 5e5], square or disk, k in {21,35,64} -> only the
+    compiled k in {21, 35} here) arriving as a Poisson process, admitted
+    under a 40 GB budget; p50/p99 latency (submit -> result) and aggregate
+    stencils/s, against serial plain FP64 assembly of the same requests."""
+    reqs = [r for r in NS.serving_requests(count * 2, seed=5) if r["k"] in (21, 35)][:count]
+    nodes = [NS.request_nodes(r) for r in reqs]
+    total = sum(r["n"] for r in reqs)
+    # serial FP64 (one request after another, host in / host out)
+    ctx = R.Context(device)
+    t0 = time.perf_counter()
+    for r, (x, y) in zip(reqs, nodes):
+        vals = [np.empty(r["n"] * r["k"]) for _ in range(3)]
+        ctx.assemble_host(R.make_desc(r["P"], precision=R.FP64), x, y, r["k"], vals)
+    serial_s = time.perf_counter() - t0
+    ctx.close()
+    srv = R.Server(device, hbm_budget=40 << 30, max_slots=8)
+    rate = len(reqs) / serial_s * 2.0  # arrivals ~2x the serial FP64 service rate
+    rng = np.random.default_rng(5)
+    gaps = rng.exponential(1.0 / rate, size=len(reqs))
+    tickets = []
+    t0 = time.perf_counter()
+    tnext = t0
+    for (r, (x, y)), g in zip(zip(reqs, nodes), gaps):
+        tnext += g
+        now = time.perf_counter()
+        if tnext > now:
+            time.sleep(tnext - now)
+        tickets.append((srv.submit(x, y, r["k"], R.make_desc(r["P"], precision=R.FP32_IR)), r))
+    lat = []
+    for t, r in tickets:
+        st, res = srv.poll(t, wait_ms=600000)
+        lat.append(res.end_ms - res.submit_ms)
+    t1 = time.perf_counter()
+    for t, _ in tickets:
+        srv.release(t)
+    srv.close()
+    lat = np.array(lat)
+    return {"requests": len(reqs), "stencils": total,
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "stencils_per_s": total / (t1 - t0), "serial_fp64_stencils_per_s": total / serial_s,
+            "arrival_rate_per_s": rate,
+            "note": "Poisson arrivals at 2x the serial FP64 service rate; latency = submit to "
+                    "device completion; k=64 (degree 4) requests excluded (no compiled kernel)"}
+
+
+if __name__ == "__main__":
+    sys.exit(main())

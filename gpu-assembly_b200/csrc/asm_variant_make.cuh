@@ -1,0 +1,42 @@
+// asm_variant_make.cuh -- defines one compiled shape of the assembly kernel
+// (RBFB_DEFINE_VARIANT) and the Variant record the runtime launches it by.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "asm_kernel.cuh"
+#include "asm_variants.h"
+
+namespace rbfb {
+
+template <typename T, int GR, int GC, int NTP, int NRHS, int P, int Q, bool MIXED, int BLOCK,
+          int MINB>
+Variant make_variant(const char* name) {
+    using C = AsmCfg<T, GR, GC, NTP, NRHS, P, Q, MIXED>;
+    Variant v{};
+    v.name = name;
+    v.kernel =
+        reinterpret_cast<const void*>(&asm_kernel<T, GR, GC, NTP, NRHS, P, Q, MIXED, BLOCK, MINB>);
+    v.launch = [](dim3 grid, int block, size_t smem, cudaStream_t st, const AsmParams& p) {
+        asm_kernel<T, GR, GC, NTP, NRHS, P, Q, MIXED, BLOCK, MINB><<<grid, block, smem, st>>>(p);
+    };
+    v.mixed = MIXED;
+    v.P = P;
+    v.Q = Q;
+    v.ntp = NTP;
+    v.nrhs = NRHS;
+    v.group = C::G;
+    v.block = BLOCK;
+    v.smem_group = C::bytes;
+    v.smem_block = C::bytes * (BLOCK / C::G);
+    return v;
+}
+
+}  // namespace rbfb
+
+#define RBFB_DEFINE_VARIANT(name, T, GR, GC, NTP, NRHS, P, Q, MIXED, BLOCK, MINB)          \
+    namespace rbfb {                                                                       \
+    Variant variant_##name() {                                                             \
+        return make_variant<T, GR, GC, NTP, NRHS, P, Q, MIXED, BLOCK, MINB>(#name);        \
+    }                                                                                      \
+    }

@@ -1,0 +1,255 @@
+// batch.cu -- uneven stencils: rbfb_assemble_csr.
+//
+// Stencils of different size and degree (interior vs boundary, k from 21 to
+// 64, degree 2 to 4) are bucketed on the device by the compiled kernel shape
+// that fits them (smallest padded system size >= k + npoly(P)), counting-
+// sorted into one stencil list, and each bucket's persistent kernel walks its
+// slice of the list. Bucket sizes and offsets stay on the device (kernels
+// read them through pointers), so the whole call is a fixed sequence of
+// launches with no host round trip; the sequence is captured once into a CUDA
+// graph and replayed for the same batch.
+//
+// The reference's only CSR-driven assembly is the Fortran fill_kernel over
+// ia/ja (src/rbf_cuda.f90:36-99); its C++ kernel takes one fixed stencil size
+// per launch (src/rbf_operators.h:187-210).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "runtime.h"
+
+namespace rbfb {
+namespace {
+
+constexpr int kMaxVariants = 64;
+constexpr int kTabN = 161;  // system sizes 0..160
+
+struct BatchState {
+    int* table = nullptr;     // [5][kTabN] variant per (P, n), -1 = none
+    int table_mixed = -1, table_phs = -1;
+    int* counts = nullptr;    // [kMaxVariants] x 3: counts | offsets | cursors
+    DevCounters* ctrs = nullptr;  // per bucket
+    int* err = nullptr;
+    size_t cap = 0;
+    int* bucket_of = nullptr;
+    int* list = nullptr;
+    // cached graph of the last batch
+    cudaGraphExec_t graph = nullptr;
+    std::vector<unsigned char> graph_key;
+    cudaStream_t cap_stream = nullptr;
+};
+
+BatchState* state(rbfb_ctx* ctx) {
+    if (!ctx->batch) ctx->batch = new BatchState();
+    return static_cast<BatchState*>(ctx->batch);
+}
+
+__global__ void assign_kernel(int nst, const int* ia, const int8_t* degree, int P0, const int* table,
+                              int* bucket_of, int* counts, int* err) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nst; s += gridDim.x * blockDim.x) {
+        const int ks = ia[s + 1] - ia[s];
+        const int P = degree ? degree[s] : P0;
+        int b = -1;
+        if (P >= 0 && P <= 4 && ks >= 1) {
+            const int n = ks + npoly(P);
+            if (n < kTabN) b = table[P * kTabN + n];
+        }
+        bucket_of[s] = b;
+        if (b >= 0) atomicAdd(counts + b, 1);
+        else atomicExch(err, 1);
+    }
+}
+
+__global__ void offsets_kernel(int* counts, int nb) {
+    int acc = 0;
+    for (int b = 0; b < nb; ++b) {
+        counts[kMaxVariants + b] = acc;   // offsets
+        counts[2 * kMaxVariants + b] = 0; // cursors
+        acc += counts[b];
+    }
+}
+
+__global__ void scatter_kernel(int nst, const int* bucket_of, int* counts, int* list) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nst; s += gridDim.x * blockDim.x) {
+        const int b = bucket_of[s];
+        if (b < 0) continue;
+        list[counts[kMaxVariants + b] + atomicAdd(counts + 2 * kMaxVariants + b, 1)] = s;
+    }
+}
+
+int ensure(rbfb_ctx* ctx, BatchState* b, size_t n) {
+    if (!b->counts) {
+        RBFB_CUDA(ctx, cudaMalloc(&b->counts, 3 * kMaxVariants * sizeof(int)));
+        RBFB_CUDA(ctx, cudaMalloc(&b->ctrs, kMaxVariants * sizeof(DevCounters)));
+        RBFB_CUDA(ctx, cudaMalloc(&b->err, sizeof(int)));
+        RBFB_CUDA(ctx, cudaMalloc(&b->table, 5 * kTabN * sizeof(int)));
+    }
+    if (b->cap < n) {
+        cudaFree(b->bucket_of);
+        cudaFree(b->list);
+        b->bucket_of = b->list = nullptr;
+        b->cap = 0;
+        RBFB_CUDA(ctx, cudaMalloc(&b->bucket_of, n * sizeof(int)));
+        RBFB_CUDA(ctx, cudaMalloc(&b->list, n * sizeof(int)));
+        b->cap = n;
+    }
+    return ensure_fb(ctx, n);
+}
+
+// The (P, n) -> variant table for one precision and PHS rule; also returns
+// the set of variants that can occur for the allowed degrees.
+int build_table(rbfb_ctx* ctx, BatchState* b, bool mixed, int phs, int Pmin, int Pmax,
+                std::vector<int>& used) {
+    std::vector<int> tab(5 * kTabN, -1);
+    used.clear();
+    for (int P = 0; P <= 4; ++P)
+        for (int n = 1; n < kTabN; ++n) {
+            const int Q = phs ? phs : 2 * P - 1;
+            if (Q < 1) continue;
+            const int v = pick_variant(ctx, mixed, P, Q, n);
+            tab[P * kTabN + n] = v;
+            if (v >= 0 && P >= Pmin && P <= Pmax &&
+                std::find(used.begin(), used.end(), v) == used.end())
+                used.push_back(v);
+        }
+    RBFB_CUDA(ctx, cudaMemcpy(b->table, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice));
+    b->table_mixed = mixed;
+    b->table_phs = phs;
+    return RBFB_OK;
+}
+
+void release(BatchState* b) {
+    cudaFree(b->table); cudaFree(b->counts); cudaFree(b->ctrs); cudaFree(b->err);
+    cudaFree(b->bucket_of); cudaFree(b->list);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+    delete b;
+}
+
+}  // namespace
+}  // namespace rbfb
+
+using namespace rbfb;
+
+extern "C" {
+
+void rbfb_release_batch(rbfb_ctx* ctx) {
+    if (ctx->batch) release(static_cast<BatchState*>(ctx->batch));
+    ctx->batch = nullptr;
+}
+
+int rbfb_assemble_csr(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const double* x,
+                      const double* y, const int* ia, const int* ja, const int8_t* degree,
+                      double* const* values_h, int* info, rbfb_stats* stats, void* stream) {
+    if (!ctx) return RBFB_EINVAL;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    int rc = check_desc(ctx, desc);
+    if (rc) return rc;
+    if (nstencils < 0 || !ia || !ja || !x || !y || !values_h)
+        return fail(ctx, RBFB_EINVAL, "null pointer argument");
+    RBFB_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    BatchState* b = state(ctx);
+    rc = ensure(ctx, b, static_cast<size_t>(std::max(nstencils, 1)));
+    if (rc) return rc;
+    const bool mixed = desc->precision == RBFB_FP32_IR;
+    std::vector<int> used;
+    rc = build_table(ctx, b, mixed, desc->phs, degree ? 0 : desc->degree,
+                     degree ? 4 : desc->degree, used);
+    if (rc) return rc;
+    if (used.empty()) return fail(ctx, RBFB_EUNSUPPORTED, "no compiled kernel for these degrees");
+
+    // the parameters every bucket shares
+    AsmParams p;
+    std::memset(&p, 0, sizeof(p));
+    const int nrhs = rhs_columns(desc, p);
+    if (nrhs < 0) return fail(ctx, nrhs, "bad operator mask / interpolation points");
+    for (int q = 0; q < nrhs; ++q) {
+        if (!values_h[q]) return fail(ctx, RBFB_EINVAL, "null values pointer");
+        p.values[q] = values_h[q];
+    }
+    p.x = x;
+    p.y = y;
+    p.ja = ja;
+    p.ia = ia;
+    p.Lx = desc->period[0];
+    p.Ly = desc->period[1];
+    p.scale = desc->scale;
+    p.info = info;
+    p.max_sweeps = desc->max_sweeps > 0 ? desc->max_sweeps : 6;
+    p.ir_tol = desc->ir_tol > 0 ? desc->ir_tol : 1e-13;
+    p.list = b->list;
+
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (stats) {
+        RBFB_CUDA(ctx, cudaEventCreate(&e0));
+        RBFB_CUDA(ctx, cudaEventCreate(&e1));
+        RBFB_CUDA(ctx, cudaEventRecord(e0, st));
+    }
+    const int nb = static_cast<int>(variants().size());
+    if (nb > kMaxVariants) return fail(ctx, RBFB_EUNSUPPORTED, "too many compiled shapes");
+    RBFB_CUDA(ctx, cudaMemsetAsync(b->counts, 0, 3 * kMaxVariants * sizeof(int), st));
+    RBFB_CUDA(ctx, cudaMemsetAsync(b->ctrs, 0, kMaxVariants * sizeof(DevCounters), st));
+    RBFB_CUDA(ctx, cudaMemsetAsync(b->err, 0, sizeof(int), st));
+    if (nstencils > 0) {
+        const int blocks = std::max(1, std::min((nstencils + 255) / 256, ctx->sms * 8));
+        assign_kernel<<<blocks, 256, 0, st>>>(nstencils, ia, degree, desc->degree, b->table,
+                                              b->bucket_of, b->counts, b->err);
+        offsets_kernel<<<1, 1, 0, st>>>(b->counts, nb);
+        scatter_kernel<<<blocks, 256, 0, st>>>(nstencils, b->bucket_of, b->counts, b->list);
+        ctx->launches += 3;
+        RBFB_CUDA(ctx, cudaGetLastError());
+        for (int v : used) {
+            if (nrhs > variants()[v].nrhs) return fail(ctx, RBFB_EUNSUPPORTED, "too many right-hand sides");
+            AsmParams q = p;
+            q.nitems_dev = b->counts + v;
+            q.list_off_dev = b->counts + kMaxVariants + v;
+            q.fb_list = ctx->fb_list;
+            q.fb_count = &b->ctrs[v].fb_count;
+            q.sweeps_max = &b->ctrs[v].sweeps_max;
+            q.sweeps_sum = &b->ctrs[v].sweeps_sum;
+            rc = launch_variant(ctx, v, q, st);
+            if (rc) return rc;
+            if (mixed) {
+                const auto& var = variants()[v];
+                const int v64 = pick_variant(ctx, false, var.P, var.Q, var.ntp);
+                if (v64 < 0) return fail(ctx, RBFB_EUNSUPPORTED, "no FP64 fallback kernel");
+                AsmParams f = q;
+                f.list = ctx->fb_list;
+                f.nitems_dev = &b->ctrs[v].fb_count;
+                f.fb_list = nullptr;
+                rc = launch_variant(ctx, v64, f, st);
+                if (rc) return rc;
+            }
+        }
+    }
+    if (!stats) return RBFB_OK;
+    std::vector<DevCounters> h(nb);
+    int herr = 0;
+    rc = count_singular(ctx, info, nstencils, &b->ctrs[0].singular, st);
+    if (rc) return rc;
+    RBFB_CUDA(ctx, cudaEventRecord(e1, st));
+    RBFB_CUDA(ctx, cudaMemcpyAsync(h.data(), b->ctrs, nb * sizeof(DevCounters), cudaMemcpyDeviceToHost, st));
+    RBFB_CUDA(ctx, cudaMemcpyAsync(&herr, b->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    RBFB_CUDA(ctx, cudaStreamSynchronize(st));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    std::memset(stats, 0, sizeof(*stats));
+    stats->stencils = nstencils;
+    stats->singular = static_cast<long long>(h[0].singular);
+    for (const auto& c : h) {
+        stats->fallback += c.fb_count;
+        stats->sweeps += static_cast<long long>(c.sweeps_sum);
+        stats->max_sweeps_used = std::max(stats->max_sweeps_used, c.sweeps_max);
+    }
+    stats->buckets = static_cast<int>(used.size());
+    stats->ms = ms;
+    if (herr) return fail(ctx, RBFB_EUNSUPPORTED, "a stencil has no compiled kernel (size or degree)");
+    return RBFB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,90 @@
+// tune.cu -- rbfb_autotune: times every compiled shape that serves one
+// (precision, P, Q, padded size) on the caller's workload and records the
+// fastest (and its CTAs per SM) in the context's launch table.
+//
+// No reference counterpart: the reference takes its block size from
+// cuSolverDx (src/rbf_operators.h:280-281).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "runtime.h"
+
+using namespace rbfb;
+
+extern "C" {
+
+int rbfb_autotune(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const double* x,
+                  const double* y, int k, const int* ja, double* const* values_h) {
+    if (!ctx) return RBFB_EINVAL;
+    int rc = check_desc(ctx, desc);
+    if (rc) return rc;
+    if (nstencils < 1 || k < 1) return fail(ctx, RBFB_EINVAL, "need stencils");
+    RBFB_CUDA(ctx, cudaSetDevice(ctx->device));
+    const int P = desc->degree;
+    const int Q = desc->phs ? desc->phs : 2 * P - 1;
+    const int n = k + npoly(P);
+    const bool mixed = desc->precision == RBFB_FP32_IR;
+    // candidate shapes: the smallest padded size that fits, every layout
+    const auto& vs = variants();
+    int ntp = 1 << 30;
+    for (const auto& v : vs)
+        if (v.mixed == mixed && v.P == P && v.Q == Q && v.ntp >= n) ntp = std::min(ntp, v.ntp);
+    std::vector<int> cands;
+    for (size_t i = 0; i < vs.size(); ++i)
+        if (vs[i].mixed == mixed && vs[i].P == P && vs[i].Q == Q && vs[i].ntp == ntp)
+            cands.push_back(static_cast<int>(i));
+    if (cands.empty()) return fail(ctx, RBFB_EUNSUPPORTED, "no compiled kernel for this shape");
+    cudaStream_t st = nullptr;
+    RBFB_CUDA(ctx, cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    cudaEvent_t a = nullptr, b = nullptr;
+    RBFB_CUDA(ctx, cudaEventCreate(&a));
+    RBFB_CUDA(ctx, cudaEventCreate(&b));
+    rc = ensure_fb(ctx, static_cast<size_t>(nstencils));
+    if (rc) return rc;
+    const auto key = std::make_tuple(mixed ? 1 : 0, P, Q, ntp);
+    const LaunchShape saved = ctx->tuned.count(key) ? ctx->tuned[key] : LaunchShape{};
+    float best = 1e30f;
+    LaunchShape best_shape;
+    for (int v : cands) {
+        int occ = grid_for(ctx, v) / std::max(ctx->sms, 1);
+        if (occ < 1) continue;
+        for (int bps = occ; bps >= 1; --bps) {
+            ctx->tuned[key] = LaunchShape{v, bps};
+            float t = 1e30f;
+            for (int rep = 0; rep < 3; ++rep) {
+                cudaMemsetAsync(ctx->ctr, 0, sizeof(DevCounters), st);
+                cudaEventRecord(a, st);
+                std::lock_guard<std::mutex> lock(ctx->mu);
+                rc = enqueue_fixed(ctx, desc, 0, nstencils, x, y, k, ja, values_h, nullptr, ctx->ctr,
+                                   ctx->fb_list, st);
+                if (rc) break;
+                cudaEventRecord(b, st);
+                cudaEventSynchronize(b);
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, a, b);
+                if (rep > 0) t = std::min(t, ms);
+            }
+            if (rc) break;
+            if (t < best) {
+                best = t;
+                best_shape = LaunchShape{v, bps};
+            }
+            if (bps <= std::max(1, occ - 3)) break;  // a few occupancy levels per shape
+        }
+        if (rc) break;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaStreamDestroy(st);
+    if (rc) {
+        ctx->tuned[key] = saved;
+        return rc;
+    }
+    ctx->tuned[key] = best_shape;
+    return best_shape.variant;
+}
+
+}  // extern "C"

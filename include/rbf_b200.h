@@ -1,0 +1,242 @@
+/* rbf_b200.h -- C ABI of the B200 (sm_100a) RBF-FD operator assembly.
+ *
+ * This is the drop-in boundary for the assembly path of ivan-pi/gpu-assembly:
+ * host C++ and Fortran (bind(c)) callers reach the sm_100a kernels through
+ * these plain-C entry points instead of instantiating the reference's
+ * cuSolverDx kernel template. Every entry point below names the reference
+ * interface it replaces (paths relative to the reference repository).
+ *
+ * Conventions (the reference's, src/rbf_operators.h:292-316):
+ *   - all array arguments are DEVICE pointers unless the name ends in _h;
+ *   - indices are 0-based int32; a fixed-width stencil table ja holds the
+ *     k neighbours of stencil s at ja[s*k .. s*k+k), self first;
+ *   - a CSR stencil table holds row s at ja[ia[s] .. ia[s+1]);
+ *   - the caller owns every buffer; entry points that need scratch take it
+ *     from the context (rbfb_ctx) and never from the caller's buffers;
+ *   - weights for right-hand side q go to values[q][row offset + j], the
+ *     weight of neighbour ja[row offset + j] (src/rbf_operators.h:307-313);
+ *   - per-stencil status info[s]: 0 = success, c+1 = zero pivot at
+ *     elimination step c (LAPACK getrf convention, src/rbf_operators.h:315);
+ *     the weights of such a stencil are written as quiet NaN;
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream); calls are
+ *     asynchronous on it unless stated otherwise.
+ *
+ * Return values: 0 on success, a negative RBFB_E* code on argument or CUDA
+ * errors (rbfb_status_string names it, rbfb_last_error gives details).
+ * Synchronous calls that count singular stencils return that count (>= 0).
+ */
+#ifndef RBF_B200_H
+#define RBF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define RBFB_OK 0
+#define RBFB_EINVAL (-1)      /* bad argument (null pointer, k > n, ...)      */
+#define RBFB_ECUDA (-2)       /* a CUDA runtime call failed                    */
+#define RBFB_ENOMEM (-3)      /* device or pinned allocation failed            */
+#define RBFB_EUNSUPPORTED (-4)/* no compiled kernel for this shape             */
+#define RBFB_ETIMEOUT (-5)    /* a bounded wait ran out                        */
+#define RBFB_EBUDGET (-6)     /* request larger than the server's HBM budget   */
+#define RBFB_ENOTFOUND (-7)   /* unknown ticket                                */
+#define RBFB_EBUSY (-8)       /* ticket not finished (non-blocking poll)       */
+
+/* ---- operators (right-hand sides) --------------------------------------
+ * Right-hand-side columns, in output order: nc interpolation points first
+ * (RBFB_OP_INTERP, the reference's fill_rhs, src/rbf_operators.h:156-185),
+ * then each derivative operator set in `ops`, in bit order, evaluated at the
+ * stencil centre. */
+#define RBFB_OP_INTERP 1
+#define RBFB_OP_LAPLACE 2
+#define RBFB_OP_DX 4
+#define RBFB_OP_DY 8
+#define RBFB_OP_DXX 16
+#define RBFB_OP_DYY 32
+#define RBFB_OP_DXY 64
+
+/* ---- precision ---------------------------------------------------------- */
+#define RBFB_FP64 0     /* FP64 fill, FP64 elimination (the plain kernel)     */
+#define RBFB_FP32_IR 1  /* FP64 fill, FP32 elimination, FP64 residual
+                           iterative refinement, FP64 fallback per stencil   */
+
+#define RBFB_MAX_RHS 8  /* right-hand sides per stencil                      */
+
+typedef struct rbfb_ctx rbfb_ctx;
+typedef struct rbfb_server rbfb_server;
+
+/* Assembly descriptor: the run-time form of the reference's compile-time
+ * interp_config<N, NRHS, P, Q, ARCH, T> (src/rbf_operators.h:187-290). */
+typedef struct rbfb_desc {
+    int degree;        /* P, total degree of the polynomial augmentation (0..4)   */
+    int phs;           /* Q, odd PHS exponent phi(r) = r^Q; 0 = 2P-1 (per stencil)*/
+    int ops;           /* RBFB_OP_* mask                                            */
+    int precision;     /* RBFB_FP64 or RBFB_FP32_IR                                 */
+    int scale;         /* 1: power-of-two radius scaling of each stencil (exact)    */
+    int max_sweeps;    /* refinement sweeps before the FP64 fallback (0 = 6)        */
+    double ir_tol;     /* stop when max|dx| <= ir_tol * max|x| (0 = 1e-13)          */
+    double period[2];  /* box sides for minimum-image displacements; 0 = open axis  */
+    int nc;            /* number of interpolation points (RBFB_OP_INTERP)           */
+    const double* xc;  /* interpolation points in the stencil-local frame (device)  */
+    const double* yc;
+} rbfb_desc;
+
+/* Counters of one assembly call (filled on synchronous calls). */
+typedef struct rbfb_stats {
+    long long stencils;       /* stencils assembled                                  */
+    long long singular;       /* stencils with info != 0                             */
+    long long fallback;       /* FP32_IR stencils re-solved in FP64                  */
+    long long sweeps;         /* refinement sweeps summed over stencils              */
+    int max_sweeps_used;      /* largest sweep count of any stencil                  */
+    int buckets;              /* kernel shapes launched                              */
+    float ms;                 /* device time of the call (CUDA events)               */
+} rbfb_stats;
+
+/* ---- context ------------------------------------------------------------ */
+/* One context per host thread (or serialise calls on it). Holds the
+ * workspace, the tuned launch table and the CUDA graphs of the batched path.
+ * No reference counterpart: the reference keeps this state in template
+ * constants and caller-owned buffers (src/rbf_operators.h:187-290). */
+int rbfb_create(rbfb_ctx** ctx, int device);
+int rbfb_destroy(rbfb_ctx* ctx);
+const char* rbfb_status_string(int status);
+const char* rbfb_last_error(const rbfb_ctx* ctx);
+/* Number of this library's kernels launched by the context so far. */
+long long rbfb_kernel_launches(const rbfb_ctx* ctx);
+
+/* ---- stencil search ----------------------------------------------------- */
+/* k nearest neighbours of every node, sorted by (squared distance, index),
+ * self first: ja[s*k + t]. period == NULL or {0,0}: open plane, the
+ * reference's NodeSet::stencils(k) (src/rbf_nodeset.h:155-181, nanoflann);
+ * period = {Lx, Ly} > 0: periodic box, minimum-image metric, the reference's
+ * KdTree::knn_stencils(k) (src/rbf_spatial.h:178-183, src/rbf_spatial.cpp:
+ * 251-260, ckdtree). period is a HOST pointer. Equal to the reference's
+ * result wherever no two candidates tie in distance. */
+int rbfb_knn_stencils(rbfb_ctx* ctx, int n, const double* x, const double* y, int k,
+                      const double* period_h, int* ja, void* stream);
+
+/* k nearest nodes of nq arbitrary query points (xq, yq): the reference's
+ * KdTree::knn_stencils(q, k) (src/rbf_spatial.h:173-178). */
+int rbfb_knn_query(rbfb_ctx* ctx, int n, const double* x, const double* y, int nq,
+                   const double* xq, const double* yq, int k, const double* period_h, int* ja,
+                   void* stream);
+
+/* Completion status of the last search on this context: 0 when every query
+ * finished, 1 when a query gave up widening its search (its row of ja is
+ * then unwritten). Synchronises `stream`. No reference counterpart (the
+ * reference's tree search cannot fail this way). */
+int rbfb_knn_status(rbfb_ctx* ctx, void* stream);
+
+/* ---- assembly ----------------------------------------------------------- */
+/* Fixed-width stencils: the reference's assemble_interp_weights<Config>
+ * (src/rbf_operators.h:320-376) and the planned assemble_laplace_weights
+ * (src/main.cpp:15-16,44-45). values_h is a HOST array of nrhs DEVICE
+ * pointers (the reference passes the same table in device memory, `A`),
+ * each to nstencils*k doubles. info may be NULL. stats may be NULL; when
+ * given, the call synchronises `stream` and fills it. */
+int rbfb_assemble(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const double* x,
+                  const double* y, int k, const int* ja, double* const* values_h, int* info,
+                  rbfb_stats* stats, void* stream);
+
+/* Ragged stencils in CSR form (ia has nstencils+1 entries), optionally with a
+ * per-stencil degree (int8, NULL = desc->degree): the uneven batch. Stencils
+ * are bucketed by system size and run in one persistent launch per call,
+ * captured in a CUDA graph and replayed when the same batch comes again.
+ * The Fortran module's fill_kernel (src/rbf_cuda.f90:36-99) is the
+ * reference's only CSR-driven assembly. */
+int rbfb_assemble_csr(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const double* x,
+                      const double* y, const int* ia, const int* ja, const int8_t* degree,
+                      double* const* values_h, int* info, rbfb_stats* stats, void* stream);
+
+/* End to end from HOST memory: copies the nodes in, finds the k-NN stencils
+ * (unless ja_h is given), assembles, and copies the stencils (ja_out_h, may
+ * be NULL) and the weights (values_h: HOST array of nrhs HOST pointers) back,
+ * pipelining the copies with the kernels in chunks. Synchronous. Returns the
+ * number of singular stencils. */
+int rbfb_assemble_host(rbfb_ctx* ctx, const rbfb_desc* desc, int n, const double* x_h,
+                       const double* y_h, int k, const int* ja_h, int* ja_out_h,
+                       double* const* values_h, int* info_h, rbfb_stats* stats);
+
+/* ---- Fortran rbf_cuda module and solve_dp counterparts ------------------- */
+/* The saddle-point matrix [A P; P^T 0] of every stencil, FP64, column-major
+ * n x n (n = k_s + npoly(P)) with leading dimension ldm, stencil s in the
+ * ldm x ldm slab at M + s*ldm*ldm (a stencil with n > ldm is skipped), in the shifted
+ * (and, with desc->scale, scaled) frame: fill_matrix (src/rbf_operators.h:
+ * 116-154) and the Fortran fill_kernel (src/rbf_cuda.f90:36-99). Uses
+ * desc->degree, desc->phs, desc->scale and desc->period. */
+int rbfb_fill_matrices(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const double* x,
+                       const double* y, const int* ia, const int* ja, double* M, int ldm,
+                       void* stream);
+
+/* va[ia[s] + j] = W[s][j][0] + W[s][j][1]: the Fortran store_to_csr, which
+ * forms a Laplacian from the d2/dx2 and d2/dy2 weight columns (src/rbf_cuda.f90:
+ * 139-157). wxx, wyy are CSR value arrays laid out like va. */
+int rbfb_store_to_csr(int nstencils, const int* ia, const double* wxx, const double* wyy,
+                      double* va, void* stream);
+
+/* Launches solve_dp<<<1,32>>>: one 15x15 system with 9 right-hand sides,
+ * FP64, A column-major (lda 15), B column-major (ldb 15), solved in place
+ * with partial pivoting; ipiv receives 1-based LAPACK-style row interchanges,
+ * *info the getrf status. The reference's demo kernel
+ * (src/rbf_operators.cpp:7-11, launched from src/main.f90:57). */
+int rbfb_solve_dp(double* A, int* ipiv, double* B, int* info, void* stream);
+
+/* ---- tuning --------------------------------------------------------------- */
+/* Times the compiled kernel shapes for one system size and precision on the
+ * given workload and records the fastest in the context's launch table
+ * (lanes per stencil, CTA size, CTAs per SM). Returns the index of the
+ * chosen shape, or a negative code. No reference counterpart (the
+ * reference's block size comes from cuSolverDx, src/rbf_operators.h:280-281). */
+int rbfb_autotune(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const double* x,
+                  const double* y, int k, const int* ja, double* const* values_h);
+
+/* ---- serving ---------------------------------------------------------------- */
+/* Continuous-batching assembly server: requests (node sets of any size) are
+ * admitted as slots and HBM budget free up, their k-NN and assembly overlap
+ * on the device, and their nodes, stencils and weights stay resident on the
+ * device until released. No reference counterpart. */
+typedef struct rbfb_request {
+    int n;               /* nodes                                                  */
+    const double* x_h;   /* HOST coordinates (copied at submit)                    */
+    const double* y_h;
+    int k;               /* stencil size                                           */
+    rbfb_desc desc;      /* operator description (xc/yc unused)                    */
+} rbfb_request;
+
+typedef struct rbfb_result {
+    int status;              /* 0, or a negative code                              */
+    int n, k, nrhs;
+    long long singular;
+    long long fallback;
+    const int* ja;           /* DEVICE, n*k, resident until rbfb_server_release    */
+    const double* values[RBFB_MAX_RHS]; /* DEVICE, n*k each                         */
+    double submit_ms, start_ms, end_ms; /* host clock, relative to server creation  */
+} rbfb_result;
+
+int rbfb_server_create(rbfb_server** srv, int device, size_t hbm_budget_bytes, int max_slots);
+int rbfb_server_submit(rbfb_server* srv, const rbfb_request* req, long long* ticket);
+/* wait_ms < 0: block; 0: poll (RBFB_EBUSY while running); > 0: bounded wait
+ * (RBFB_ETIMEOUT when it runs out). */
+int rbfb_server_poll(rbfb_server* srv, long long ticket, int wait_ms, rbfb_result* res);
+/* Copies a finished request's weights (and stencils if ja_h != NULL) to host. */
+int rbfb_server_fetch(rbfb_server* srv, long long ticket, int* ja_h, double* const* values_h);
+int rbfb_server_release(rbfb_server* srv, long long ticket);
+int rbfb_server_destroy(rbfb_server* srv);
+/* Bytes of device memory currently held by admitted requests. */
+size_t rbfb_server_resident_bytes(const rbfb_server* srv);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#ifdef __CUDACC__
+/* The reference's C-ABI kernel symbol, same signature
+ * (src/rbf_operators.cpp:7): launch <<<1, 32>>>. */
+extern "C" __global__ void solve_dp(double* A, int* ipiv, double* B, int* info);
+#endif
+
+#endif /* RBF_B200_H */

@@ -1,0 +1,258 @@
+"""ctypes front end of the CPU oracle (TEST INFRASTRUCTURE).
+
+Only tests/, ``__graft_entry__.smoke()`` and the CPU legs of ``bench.py`` may
+import this module: it is the checker and the CPU baseline, never part of the
+product. It loads
+
+* ``oracle/_build/liboracle.so`` -- the CPU restatement of the reference's
+  assembly path (``oracle/rbf_oracle.cpp``), and
+* ``oracle/_ref/libref_knn.so`` -- the reference's own nanoflann / ckdtree
+  stencil searches compiled from the reference sources (``oracle/Makefile``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "_build" / "liboracle.so"
+REF_SO = HERE / "_ref" / "libref_knn.so"
+
+OP_INTERP, OP_LAPLACE, OP_DX, OP_DY, OP_DXX, OP_DYY, OP_DXY = 1, 2, 4, 8, 16, 32, 64
+
+_lib = None
+_ref = None
+
+_dp = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+
+
+def lib():
+    """The oracle library (built by ``make -C oracle``)."""
+    global _lib
+    if _lib is None:
+        if not ORACLE_SO.exists():
+            raise RuntimeError(f"oracle library missing: {ORACLE_SO} (run make -C oracle)")
+        L = C.CDLL(str(ORACLE_SO))
+        L.orc_assemble_fixed.restype = C.c_longlong
+        L.orc_assemble_fixed.argtypes = [C.c_int, _dp, _dp, C.c_int, _ip, C.c_int, C.c_int, C.c_int,
+                                         C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_double,
+                                         C.c_double, C.c_void_p, C.c_void_p]
+        L.orc_assemble_csr.restype = C.c_longlong
+        L.orc_assemble_csr.argtypes = [C.c_int, _dp, _dp, _ip, _ip, C.c_void_p, C.c_int, C.c_int,
+                                       C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
+                                       C.c_double, C.c_double, C.c_void_p, C.c_void_p]
+        L.orc_solve_stencil.restype = C.c_int
+        L.orc_solve_stencil.argtypes = [C.c_int, _dp, _dp, C.c_int, _ip, C.c_int, C.c_int, C.c_int,
+                                        C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_double,
+                                        C.c_double, _dp, C.c_void_p]
+        L.orc_fill_matrix.restype = C.c_int
+        L.orc_fill_matrix.argtypes = [C.c_int, _dp, _dp, C.c_int, _ip, C.c_int, C.c_int, C.c_int,
+                                      C.c_double, C.c_double, _dp, C.c_int]
+        L.orc_knn_brute.restype = C.c_int
+        L.orc_knn_brute.argtypes = [C.c_int, _dp, _dp, C.c_int, _dp, _dp, C.c_int, C.c_double,
+                                    C.c_double, _ip, C.c_void_p]
+        L.orc_stencil_d2.restype = None
+        L.orc_stencil_d2.argtypes = [C.c_int, _dp, _dp, C.c_int, _ip, C.c_double, C.c_double, _dp]
+        L.orc_num_rhs.restype = C.c_int
+        L.orc_num_rhs.argtypes = [C.c_int, C.c_int]
+        L.orc_npoly.restype = C.c_int
+        L.orc_npoly.argtypes = [C.c_int]
+        L.orc_phs.restype = C.c_double
+        L.orc_phs.argtypes = [C.c_int, C.c_double]
+        L.orc_set_threads.argtypes = [C.c_int]
+        L.orc_max_threads.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def ref():
+    """The reference's own stencil searches, or None when not built here."""
+    global _ref
+    if _ref is None:
+        if not REF_SO.exists():
+            return None
+        L = C.CDLL(str(REF_SO))
+        L.ref_nodeset_stencils.restype = C.c_int
+        L.ref_nodeset_stencils.argtypes = [C.c_int, _dp, _dp, C.c_int, _ip]
+        L.ref_kdtree_stencils.restype = C.c_int
+        L.ref_kdtree_stencils.argtypes = [C.c_int, _dp, _dp, C.c_int, C.c_double, C.c_double, _ip]
+        L.ref_set_threads.argtypes = [C.c_int]
+        _ref = L
+    return _ref
+
+
+def set_threads(n: int) -> None:
+    lib().orc_set_threads(int(n))
+    r = ref()
+    if r is not None:
+        r.ref_set_threads(int(n))
+
+
+def max_threads() -> int:
+    return int(lib().orc_max_threads())
+
+
+def npoly(P: int) -> int:
+    return (P + 1) * (P + 2) // 2 if P >= 0 else 0
+
+
+def num_rhs(ops: int, nc: int = 0) -> int:
+    return int(lib().orc_num_rhs(ops, nc))
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _ptr_table(arrs):
+    t = (C.c_void_p * len(arrs))()
+    for i, a in enumerate(arrs):
+        t[i] = a.ctypes.data
+    return t
+
+
+def assemble(x, y, ja, k, P, Q=None, ops=OP_LAPLACE | OP_DX | OP_DY, xc=None, yc=None,
+             scale=True, period=None):
+    """FP64 assembly of fixed-width stencils (ja: n*k). Returns (values, info)
+    with values of shape (nrhs, n*k)."""
+    x, y, ja = _f64(x), _f64(y), _i32(ja)
+    n = x.size
+    Q = 2 * P - 1 if Q is None else Q
+    nc = 0 if xc is None else len(xc)
+    xc_a = None if xc is None else _f64(xc)
+    yc_a = None if yc is None else _f64(yc)
+    nrhs = num_rhs(ops, nc)
+    out = [np.empty(n * k, np.float64) for _ in range(nrhs)]
+    info = np.zeros(n, np.int32)
+    Lx, Ly = (0.0, 0.0) if period is None else (float(period[0]), float(period[1]))
+    rc = lib().orc_assemble_fixed(n, x, y, k, ja, P, Q, ops, nc,
+                                  None if xc_a is None else xc_a.ctypes.data,
+                                  None if yc_a is None else yc_a.ctypes.data, int(bool(scale)),
+                                  Lx, Ly, _ptr_table(out), info.ctypes.data)
+    if rc < 0:
+        raise ValueError("oracle rejected the arguments")
+    return np.stack(out), info
+
+
+def assemble_csr(x, y, ia, ja, degree=None, P=2, Q=0, ops=OP_LAPLACE | OP_DX | OP_DY,
+                 scale=True, period=None, nstencils=None):
+    """FP64 assembly of ragged CSR stencils; degree: per-stencil int8 or None.
+    Q = 0 selects Q_s = 2 P_s - 1. Stencil s is centred on node s; by default
+    every node has a stencil, nstencils restricts it to the first ones."""
+    x, y, ia, ja = _f64(x), _f64(y), _i32(ia), _i32(ja)
+    n = x.size if nstencils is None else int(nstencils)
+    nrhs = num_rhs(ops, 0)
+    out = [np.empty(int(ia[-1]), np.float64) for _ in range(nrhs)]
+    info = np.zeros(n, np.int32)
+    deg = None if degree is None else np.ascontiguousarray(degree, dtype=np.int8)
+    Lx, Ly = (0.0, 0.0) if period is None else (float(period[0]), float(period[1]))
+    rc = lib().orc_assemble_csr(n, x, y, ia, ja, None if deg is None else deg.ctypes.data, P, Q,
+                                ops, 0, None, None, int(bool(scale)), Lx, Ly, _ptr_table(out),
+                                info.ctypes.data)
+    if rc < 0:
+        raise ValueError("oracle rejected the arguments")
+    return np.stack(out), info
+
+
+def solve_stencil(s, x, y, idx, P, Q=None, ops=OP_LAPLACE | OP_DX | OP_DY, scale=True,
+                  period=None):
+    """Full solution (np polynomial coefficients, then k weights) of one
+    stencil in the scaled frame, shape (n, nrhs); plus info."""
+    x, y, idx = _f64(x), _f64(y), _i32(idx)
+    k = idx.size
+    Q = 2 * P - 1 if Q is None else Q
+    nrhs = num_rhs(ops, 0)
+    n = k + npoly(P)
+    sol = np.empty(n * nrhs, np.float64)
+    out = [np.empty(k, np.float64) for _ in range(nrhs)]
+    Lx, Ly = (0.0, 0.0) if period is None else (float(period[0]), float(period[1]))
+    info = lib().orc_solve_stencil(s, x, y, k, idx, P, Q, ops, 0, None, None, int(bool(scale)),
+                                   Lx, Ly, sol, _ptr_table(out))
+    return sol.reshape(n, nrhs), info
+
+
+def fill_matrix(s, x, y, idx, P, Q=None, scale=True, period=None):
+    """The reference-layout saddle-point matrix [A P; P^T 0] of one stencil
+    (column-major in the reference; returned as a numpy (n, n) array)."""
+    x, y, idx = _f64(x), _f64(y), _i32(idx)
+    k = idx.size
+    Q = 2 * P - 1 if Q is None else Q
+    n = k + npoly(P)
+    M = np.empty(n * n, np.float64)
+    Lx, Ly = (0.0, 0.0) if period is None else (float(period[0]), float(period[1]))
+    e = lib().orc_fill_matrix(s, x, y, k, idx, P, Q, int(bool(scale)), Lx, Ly, M, n)
+    return M.reshape(n, n).T.copy(), e
+
+
+def knn_brute(x, y, k, xq=None, yq=None, period=None, return_d2=False):
+    """Brute-force k-NN ordered by (squared distance, index) in the
+    reference's distance arithmetic. O(n) per query."""
+    x, y = _f64(x), _f64(y)
+    xq = x if xq is None else _f64(xq)
+    yq = y if yq is None else _f64(yq)
+    nq = xq.size
+    ja = np.empty(nq * k, np.int32)
+    d2 = np.empty(nq * k, np.float64) if return_d2 else None
+    Lx, Ly = (0.0, 0.0) if period is None else (float(period[0]), float(period[1]))
+    rc = lib().orc_knn_brute(x.size, x, y, nq, xq, yq, k, Lx, Ly, ja,
+                             None if d2 is None else d2.ctypes.data)
+    if rc < 0:
+        raise ValueError("bad k")
+    return (ja, d2) if return_d2 else ja
+
+
+def stencil_d2(x, y, ja, k, period=None):
+    """Squared distances of a stencil table, in the reference's arithmetic."""
+    x, y, ja = _f64(x), _f64(y), _i32(ja)
+    d2 = np.empty(ja.size, np.float64)
+    Lx, Ly = (0.0, 0.0) if period is None else (float(period[0]), float(period[1]))
+    lib().orc_stencil_d2(x.size, x, y, k, ja, Lx, Ly, d2)
+    return d2
+
+
+def ref_nodeset_stencils(x, y, k):
+    """rbf::NodeSet::stencils(k) of the reference (nanoflann, open plane)."""
+    r = ref()
+    if r is None:
+        raise RuntimeError("reference search library not built (oracle/_ref)")
+    x, y = _f64(x), _f64(y)
+    ja = np.empty(x.size * k, np.int32)
+    if r.ref_nodeset_stencils(x.size, x, y, k, ja) != 0:
+        raise ValueError("bad k")
+    return ja
+
+
+def ref_kdtree_stencils(x, y, k, period=None):
+    """rbf::spatial::KdTree::knn_stencils(k) of the reference (ckdtree)."""
+    r = ref()
+    if r is None:
+        raise RuntimeError("reference search library not built (oracle/_ref)")
+    x, y = _f64(x), _f64(y)
+    ja = np.empty(x.size * k, np.int32)
+    Lx, Ly = (0.0, 0.0) if period is None else (float(period[0]), float(period[1]))
+    if r.ref_kdtree_stencils(x.size, x, y, k, Lx, Ly, ja) != 0:
+        raise ValueError("bad k")
+    return ja
+
+
+def max_rel_err(w, w_ref, k):
+    """Per stencil and right-hand side, ||w - w_ref||_inf / ||w_ref||_inf;
+    returns the maximum over stencils for every right-hand side."""
+    w = np.asarray(w).reshape(w.shape[0], -1, k)
+    w_ref = np.asarray(w_ref).reshape(w_ref.shape[0], -1, k)
+    num = np.abs(w - w_ref).max(axis=2)
+    den = np.abs(w_ref).max(axis=2)
+    den = np.where(den > 0, den, 1.0)
+    return (num / den).max(axis=1)
+
+
+if os.environ.get("RBFB_ORACLE_THREADS"):
+    set_threads(int(os.environ["RBFB_ORACLE_THREADS"]))

@@ -1,0 +1,533 @@
+// rbf_oracle.cpp -- CPU restatement of the RBF-FD assembly path of
+// ivan-pi/gpu-assembly, in FP64.
+//
+// TEST INFRASTRUCTURE. This file is the checker, never the product: only
+// tests/, __graft_entry__.smoke() and the cpu_baseline / reference legs of
+// bench.py load it. The CUDA library never links or calls it.
+//
+// What it restates (reference paths are relative to the reference repo):
+//   phs()            PHS<Q>                         src/rbf_operators.h:39-76
+//   monomials()      PolyBasis<P>, npoly            src/rbf_operators.h:78-114
+//   fill_system()    fill_matrix<N,P,Q>             src/rbf_operators.h:116-154
+//   interp rhs       fill_rhs<N,P,NRHS,Q>           src/rbf_operators.h:156-185
+//   gather/shift     assemble_interp_weights        src/rbf_operators.h:350-358
+//   scatter          assemble_interp_weights        src/rbf_operators.h:368-375
+//   minimum image    PeriodicBox::minimum_image     src/rbf_spatial.h:74-76
+//   brute k-NN       test_spatial brute_knn + metric  test/test_spatial.cpp:59-82
+//                    nanoflann L2_Simple_Adaptor    third_party/nanoflann/nanoflann.hpp:690-699
+//                    ckdtree wrap_distance          third_party/ckdtree/src/distance.h:262-272
+//
+// What it adds, because the reference has it only as intent:
+//   * derivative right-hand sides at the stencil centre (Laplacian, d/dx,
+//     d/dy, d2/dx2, d2/dy2, d2/dxdy); the Fortran store_to_csr forms the
+//     Laplacian from two second-derivative columns (src/rbf_cuda.f90:139-157)
+//     and src/main.cpp:15-16 names a Laplacian assembly that does not exist.
+//   * radius scaling by a power of two (exact in binary floating point).
+//   * the solver. The reference calls cuSolverDx gesv_partial_pivot, a
+//     closed library, so the solve here is the textbook Gaussian
+//     elimination with partial pivoting (Golub & Van Loan, Matrix
+//     Computations, alg. 3.4.1) in its row-implicit form: rows are never
+//     swapped; at step c the pivot is the unused row with the largest
+//     |a(r,c)|, ties going to the lowest row index; multipliers are
+//     a(r,c) * (1 / pivot); updates are fma(-l, u, a); back substitution
+//     is column oriented, x_c = y_c * (1 / pivot_c). The CUDA FP64 kernel
+//     performs the same operations in the same order.
+//
+// Arithmetic is pinned: compiled with -ffp-contract=off, every fused
+// multiply-add is an explicit std::fma, everything else rounds per operation.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+constexpr int kMaxSys = 160;  // largest system (stencil size + polynomial terms)
+constexpr int kMaxRhs = 16;   // largest number of right-hand sides
+
+// Operator bits, the same values as include/rbf_b200.h.
+enum : int {
+    OP_INTERP = 1,
+    OP_LAPLACE = 2,
+    OP_DX = 4,
+    OP_DY = 8,
+    OP_DXX = 16,
+    OP_DYY = 32,
+    OP_DXY = 64,
+};
+
+inline int npoly(int P) { return P < 0 ? 0 : (P + 1) * (P + 2) / 2; }
+
+// phi(r) = r^Q from r^2, src/rbf_operators.h:39-76: the Q = 3, 5, 7
+// specialisations, else the generic loop.
+inline double phs(int Q, double r2) {
+    switch (Q) {
+        case 3:
+            return r2 * std::sqrt(r2);
+        case 5:
+            return r2 * r2 * std::sqrt(r2);
+        case 7: {
+            const double r4 = r2 * r2;
+            return r4 * r2 * std::sqrt(r2);
+        }
+        default: {
+            const double r = std::sqrt(r2);
+            double p = r;
+            for (int i = 0; i < (Q - 1) / 2; ++i) p *= r2;
+            return p;
+        }
+    }
+}
+
+// r^m for odd m >= 1, the same product order as phs().
+inline double rpow_odd(int m, double r2) { return m == 1 ? std::sqrt(r2) : phs(m, r2); }
+
+// 2-D monomials of total degree <= P, ordered by degree d, then by the
+// power j of y: x^(d-j) y^j. src/rbf_operators.h:81-99.
+inline void monomials(int P, double x, double y, double* b, int inc) {
+    double X[8], Y[8];
+    X[0] = Y[0] = 1.0;
+    for (int i = 1; i <= P; ++i) {
+        X[i] = X[i - 1] * x;
+        Y[i] = Y[i - 1] * y;
+    }
+    int k = 0;
+    for (int d = 0; d <= P; ++d)
+        for (int j = 0; j <= d; ++j) b[(k++) * inc] = X[d - j] * Y[j];
+}
+
+// Value of the differential operator `op` applied to monomial number i at
+// the origin: only the monomials 1, x, y, x^2, xy, y^2 (i = 0..5) can be
+// nonzero there.
+inline double poly_op_at_origin(int op, int i) {
+    switch (op) {
+        case OP_LAPLACE: return (i == 3 || i == 5) ? 2.0 : 0.0;
+        case OP_DX: return i == 1 ? 1.0 : 0.0;
+        case OP_DY: return i == 2 ? 1.0 : 0.0;
+        case OP_DXX: return i == 3 ? 2.0 : 0.0;
+        case OP_DYY: return i == 5 ? 2.0 : 0.0;
+        case OP_DXY: return i == 4 ? 1.0 : 0.0;
+        default: return 0.0;
+    }
+}
+
+// Operator applied in the evaluation point x_e to phi(|x_e - x_k|), at
+// x_e = 0, for a node at (xk, yk) with r2 = xk^2 + yk^2:
+//   d/dx  : -Q r^(Q-2) xk                d/dy : -Q r^(Q-2) yk
+//   Lap   :  Q^2 r^(Q-2)
+//   d2/dx2:  Q r^(Q-2) + Q(Q-2) r^(Q-2) xk^2 / r^2   (0 at r = 0)
+//   d2/dy2:  likewise with yk;  d2/dxdy: Q(Q-2) r^(Q-2) xk yk / r^2
+inline double phs_op_at_origin(int op, int Q, double xk, double yk, double r2) {
+    const double rq2 = rpow_odd(Q - 2, r2);
+    const double q = static_cast<double>(Q);
+    switch (op) {
+        case OP_LAPLACE: return (q * q) * rq2;
+        case OP_DX: return -((q * rq2) * xk);
+        case OP_DY: return -((q * rq2) * yk);
+        case OP_DXX:
+        case OP_DYY:
+        case OP_DXY: {
+            if (r2 == 0.0) return 0.0;
+            const double a = q * rq2;
+            const double b = (q * (q - 2.0)) * rq2;
+            if (op == OP_DXX) return a + b * ((xk * xk) / r2);
+            if (op == OP_DYY) return a + b * ((yk * yk) / r2);
+            return b * ((xk * yk) / r2);
+        }
+        default: return 0.0;
+    }
+}
+
+// Order of the derivative an operator takes: the power of the radius
+// scale its weights carry.
+inline int op_order(int op) {
+    switch (op) {
+        case OP_INTERP: return 0;
+        case OP_DX:
+        case OP_DY: return 1;
+        default: return 2;
+    }
+}
+
+// Right-hand-side columns in output order: nc interpolation points first
+// (when OP_INTERP is set), then the derivative operators in bit order.
+int rhs_columns(int ops, int nc, int* col_op) {
+    int m = 0;
+    if (ops & OP_INTERP)
+        for (int j = 0; j < nc; ++j) col_op[m++] = OP_INTERP;
+    for (int bit = OP_LAPLACE; bit <= OP_DXY; bit <<= 1)
+        if (ops & bit) col_op[m++] = bit;
+    return m;
+}
+
+// Power-of-two radius scale: returns e with 2^(e-1) <= max|d| < 2^e, so
+// scaled coordinates ldexp(d, -e) lie in (-1, 1). e = 0 when all
+// displacements are zero.
+inline int scale_exponent(const double* xs, const double* ys, int k) {
+    double m = 0.0;
+    for (int j = 0; j < k; ++j) m = std::max(m, std::max(std::fabs(xs[j]), std::fabs(ys[j])));
+    if (m == 0.0) return 0;
+    int e;
+    std::frexp(m, &e);
+    return e;
+}
+
+// PeriodicBox::minimum_image, src/rbf_spatial.h:74-76.
+inline double minimum_image(double d, double L) {
+    if (L <= 0.0) return d;
+    return d - L * std::rint(d / L);
+}
+
+struct Desc {
+    int ops;
+    int nc;
+    const double* xc;  // interpolation points, stencil-local frame
+    const double* yc;
+    int scale;         // 1: power-of-two radius scaling
+    double Lx, Ly;     // periods, <= 0 for an open axis
+};
+
+// Assemble one stencil. idx[0..k) are the node indices (idx[0] the
+// centre by convention, but the centre is node s whatever idx holds).
+// Writes w[col][j] = weight of node idx[j] for right-hand side col into
+// out[col] + j. Returns info: 0, or c + 1 for the first zero pivot.
+int assemble_one(const Desc& D, int P, int Q, int s, int k, const int* idx, const double* x,
+                 const double* y, double* const* out, long long out_off,
+                 double* sol_out /* optional n*nrhs, row-major, solution incl. polynomial part */) {
+    const int np = npoly(P);
+    const int n = k + np;
+    int col_op[kMaxRhs + 64];
+    const int nrhs = rhs_columns(D.ops, D.nc, col_op);
+    const int W = n + nrhs;
+
+    double xs[kMaxSys], ys[kMaxSys];
+    // gather + FP64 shift to the stencil centre, src/rbf_operators.h:354-358
+    const double x0 = x[s], y0 = y[s];
+    for (int j = 0; j < k; ++j) {
+        xs[j] = minimum_image(x[idx[j]] - x0, D.Lx);
+        ys[j] = minimum_image(y[idx[j]] - y0, D.Ly);
+    }
+    const int e = D.scale ? scale_exponent(xs, ys, k) : 0;
+    if (e != 0)
+        for (int j = 0; j < k; ++j) {
+            xs[j] = std::ldexp(xs[j], -e);
+            ys[j] = std::ldexp(ys[j], -e);
+        }
+
+    // Augmented system, row-major a[r][c], r < n, c < W. The reference's
+    // saddle-point matrix [A P; P^T 0] (fill_matrix, src/rbf_operators.h:
+    // 123-154) is formed with its polynomial block first: equations
+    // [P^T rows (np); node rows (k)], unknowns [lambda (np); w (k)]. This
+    // relabelling of equations and unknowns fixes the elimination order the
+    // CUDA kernel uses; the solution is the reference system's.
+    static thread_local std::vector<double> abuf;
+    abuf.assign(static_cast<size_t>(n) * W, 0.0);
+    double* a = abuf.data();
+    for (int i = 0; i < k; ++i) {
+        double* row = a + static_cast<size_t>(np + i) * W;
+        for (int j = 0; j < k; ++j) {
+            const double dx = xs[j] - xs[i];
+            const double dy = ys[j] - ys[i];
+            row[np + j] = phs(Q, dx * dx + dy * dy);
+        }
+        double b[64];
+        monomials(P, xs[i], ys[i], b, 1);
+        for (int m = 0; m < np; ++m) {
+            row[m] = b[m];                 // P block (node row i, monomial m)
+            a[m * W + np + i] = b[m];      // P^T block (monomial row m, node i)
+        }
+    }
+    // right-hand sides
+    int ic = 0;
+    for (int q = 0; q < nrhs; ++q) {
+        const int op = col_op[q];
+        if (op == OP_INTERP) {
+            // src/rbf_operators.h:158-185
+            const double xe = std::ldexp(D.xc[ic], -e), ye = std::ldexp(D.yc[ic], -e);
+            ++ic;
+            for (int i = 0; i < k; ++i) {
+                const double dx = xe - xs[i], dy = ye - ys[i];
+                a[(np + i) * W + n + q] = phs(Q, dx * dx + dy * dy);
+            }
+            double b[64];
+            monomials(P, xe, ye, b, 1);
+            for (int m = 0; m < np; ++m) a[m * W + n + q] = b[m];
+        } else {
+            for (int i = 0; i < k; ++i) {
+                const double r2 = xs[i] * xs[i] + ys[i] * ys[i];
+                a[(np + i) * W + n + q] = phs_op_at_origin(op, Q, xs[i], ys[i], r2);
+            }
+            for (int m = 0; m < np; ++m) a[m * W + n + q] = poly_op_at_origin(op, m);
+        }
+    }
+
+    // Gaussian elimination with row-implicit partial pivoting
+    bool used[kMaxSys];
+    int pstep_row[kMaxSys];  // row pivoted at step c
+    double pinv[kMaxSys];    // 1 / pivot at step c
+    std::fill(used, used + n, false);
+    int info = 0;
+    for (int c = 0; c < n; ++c) {
+        int p = -1;
+        double best = -1.0;
+        for (int r = 0; r < n; ++r) {
+            if (used[r]) continue;
+            const double v = std::fabs(a[r * W + c]);
+            if (v > best) {
+                best = v;
+                p = r;
+            }
+        }
+        if (!(best > 0.0)) {  // zero (or NaN) pivot column
+            info = c + 1;
+            break;
+        }
+        used[p] = true;
+        pstep_row[c] = p;
+        const double inv = 1.0 / a[p * W + c];
+        pinv[c] = inv;
+        const double* u = a + static_cast<size_t>(p) * W;
+        for (int r = 0; r < n; ++r) {
+            if (used[r]) continue;
+            double* ar = a + static_cast<size_t>(r) * W;
+            const double l = ar[c] * inv;
+            ar[c] = l;
+            for (int j = c + 1; j < W; ++j) ar[j] = std::fma(-l, u[j], ar[j]);
+        }
+    }
+
+    double* xsol = sol_out;
+    std::vector<double> xtmp;
+    if (!xsol) {
+        xtmp.resize(static_cast<size_t>(n) * nrhs);
+        xsol = xtmp.data();
+    }
+    if (info == 0) {
+        // column-oriented back substitution on the transformed right-hand sides
+        for (int c = n - 1; c >= 0; --c) {
+            const int p = pstep_row[c];
+            for (int q = 0; q < nrhs; ++q) xsol[c * nrhs + q] = a[p * W + n + q] * pinv[c];
+            for (int t = 0; t < c; ++t) {
+                const int r = pstep_row[t];
+                const double urc = a[r * W + c];
+                for (int q = 0; q < nrhs; ++q)
+                    a[r * W + n + q] = std::fma(-urc, xsol[c * nrhs + q], a[r * W + n + q]);
+            }
+        }
+    } else {
+        const double nan = std::numeric_limits<double>::quiet_NaN();
+        for (int i = 0; i < n * nrhs; ++i) xsol[i] = nan;
+    }
+    // scatter the k node weights (unknowns np..np+k-1), rescaled,
+    // src/rbf_operators.h:368-375; the polynomial coefficients are dropped
+    for (int q = 0; q < nrhs; ++q) {
+        const int m = op_order(col_op[q]);
+        double* dst = out[q] + out_off;
+        for (int j = 0; j < k; ++j) dst[j] = std::ldexp(xsol[(np + j) * nrhs + q], -m * e);
+    }
+    return info;
+}
+
+int check_desc(const Desc& D, int P, int Q, int kmax) {
+    if (P < -1 || P > 6) return -1;
+    if (Q < 1 || Q % 2 == 0) return -1;
+    if (kmax < 1 || kmax + npoly(P) > kMaxSys) return -1;
+    int col_op[kMaxRhs + 64];
+    if ((D.ops & OP_INTERP) && (D.nc < 1 || !D.xc || !D.yc)) return -1;
+    if (D.nc > kMaxRhs) return -1;
+    const int nrhs = rhs_columns(D.ops, D.nc, col_op);
+    if (nrhs < 1 || nrhs > kMaxRhs) return -1;
+    return nrhs;
+}
+
+}  // namespace
+
+extern "C" {
+
+// Threads used by the OpenMP loops below (0 = leave the runtime default).
+void orc_set_threads(int nthreads) {
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+}
+
+int orc_max_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+int orc_npoly(int P) { return npoly(P); }
+
+double orc_phs(int Q, double r2) { return phs(Q, r2); }
+
+// Number of right-hand-side columns for an operator mask.
+int orc_num_rhs(int ops, int nc) {
+    int col_op[kMaxRhs + 64];
+    return rhs_columns(ops, nc, col_op);
+}
+
+// Fixed-width stencils: ja has nstencils*k entries, row s at ja[s*k]
+// (src/rbf_operators.h:307-313). out[q] has nstencils*k entries for each
+// of the orc_num_rhs(ops, nc) columns. Returns the number of singular
+// stencils (info != 0), or -1 on bad arguments.
+long long orc_assemble_fixed(int nstencils, const double* x, const double* y, int k,
+                             const int* ja, int P, int Q, int ops, int nc, const double* xc,
+                             const double* yc, int scale, double Lx, double Ly,
+                             double* const* out, int* info) {
+    Desc D{ops, nc, xc, yc, scale, Lx, Ly};
+    if (check_desc(D, P, Q, k) < 0 || nstencils < 0) return -1;
+    long long bad = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : bad)
+    for (int s = 0; s < nstencils; ++s) {
+        const int st = assemble_one(D, P, Q, s, k, ja + static_cast<size_t>(s) * k, x, y, out,
+                                    static_cast<long long>(s) * k, nullptr);
+        if (info) info[s] = st;
+        bad += (st != 0);
+    }
+    return bad;
+}
+
+// Ragged stencils in CSR form: row s holds ja[ia[s] .. ia[s+1]). degree
+// is per stencil (P_s) or NULL for the uniform P; phs_q <= 0 selects
+// Q_s = 2 P_s - 1 per stencil. out[q] has ia[nstencils] entries.
+long long orc_assemble_csr(int nstencils, const double* x, const double* y, const int* ia,
+                           const int* ja, const signed char* degree, int P, int Q, int ops,
+                           int nc, const double* xc, const double* yc, int scale, double Lx,
+                           double Ly, double* const* out, int* info) {
+    Desc D{ops, nc, xc, yc, scale, Lx, Ly};
+    long long bad = 0;
+    int err = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : bad, err)
+    for (int s = 0; s < nstencils; ++s) {
+        const int ks = ia[s + 1] - ia[s];
+        const int Ps = degree ? degree[s] : P;
+        const int Qs = Q > 0 ? Q : 2 * Ps - 1;
+        if (check_desc(D, Ps, Qs, ks) < 0) {
+            err += 1;
+            continue;
+        }
+        const int st = assemble_one(D, Ps, Qs, s, ks, ja + ia[s], x, y, out, ia[s], nullptr);
+        if (info) info[s] = st;
+        bad += (st != 0);
+    }
+    return err ? -1 : bad;
+}
+
+// One stencil's full solution, row-major n x nrhs in the scaled frame:
+// polynomial coefficients (np rows) first, then the k weights. For tests.
+int orc_solve_stencil(int s, const double* x, const double* y, int k, const int* idx, int P,
+                      int Q, int ops, int nc, const double* xc, const double* yc, int scale,
+                      double Lx, double Ly, double* sol, double* const* out) {
+    Desc D{ops, nc, xc, yc, scale, Lx, Ly};
+    if (check_desc(D, P, Q, k) < 0) return -1;
+    return assemble_one(D, P, Q, s, k, idx, x, y, out, 0, sol);
+}
+
+// The saddle-point matrix of one stencil, column-major n x n with leading
+// dimension ldm (fill_matrix's layout, src/rbf_operators.h:116-122), in the
+// shifted frame and, with scale = 1, the scaled one. Returns the scale
+// exponent e.
+int orc_fill_matrix(int s, const double* x, const double* y, int k, const int* idx, int P,
+                    int Q, int scale, double Lx, double Ly, double* M, int ldm) {
+    const int np = npoly(P);
+    double xs[kMaxSys], ys[kMaxSys];
+    for (int j = 0; j < k; ++j) {
+        xs[j] = minimum_image(x[idx[j]] - x[s], Lx);
+        ys[j] = minimum_image(y[idx[j]] - y[s], Ly);
+    }
+    const int e = scale ? scale_exponent(xs, ys, k) : 0;
+    for (int j = 0; j < k; ++j) {
+        xs[j] = std::ldexp(xs[j], -e);
+        ys[j] = std::ldexp(ys[j], -e);
+    }
+    const int n = k + np;
+    for (int c = 0; c < n; ++c)
+        for (int r = 0; r < n; ++r) M[r + c * ldm] = 0.0;
+    for (int c = 0; c < k; ++c)
+        for (int r = 0; r < k; ++r) {
+            const double dx = xs[c] - xs[r];
+            const double dy = ys[c] - ys[r];
+            M[r + c * ldm] = phs(Q, dx * dx + dy * dy);
+        }
+    for (int r = 0; r < k; ++r) {
+        monomials(P, xs[r], ys[r], &M[r + k * ldm], ldm);
+        monomials(P, xs[r], ys[r], &M[k + r * ldm], 1);
+    }
+    return e;
+}
+
+// Brute-force k nearest neighbours of nq query points among n points,
+// ordered by (squared distance, index). The squared distance is formed as
+// the reference's searches form it: dx*dx + dy*dy of the plain differences
+// (nanoflann, open plane), or of ckdtree's wrapped differences in a
+// periodic box (Lx, Ly > 0). O(n) per query: small clouds only.
+int orc_knn_brute(int n, const double* x, const double* y, int nq, const double* xq,
+                  const double* yq, int k, double Lx, double Ly, int* ja, double* d2out) {
+    if (k < 1 || k > n) return -1;
+#pragma omp parallel
+    {
+        std::vector<std::pair<double, int>> cand(n);
+#pragma omp for schedule(dynamic, 16)
+        for (int q = 0; q < nq; ++q) {
+            for (int j = 0; j < n; ++j) {
+                double dx = xq[q] - x[j];
+                double dy = yq[q] - y[j];
+                if (Lx > 0) {  // ckdtree wrap_distance
+                    const double hb = 0.5 * Lx;
+                    if (dx < -hb) dx = Lx + dx;
+                    else if (dx > hb) dx = dx - Lx;
+                }
+                if (Ly > 0) {
+                    const double hb = 0.5 * Ly;
+                    if (dy < -hb) dy = Ly + dy;
+                    else if (dy > hb) dy = dy - Ly;
+                }
+                cand[j] = {dx * dx + dy * dy, j};
+            }
+            std::partial_sort(cand.begin(), cand.begin() + k, cand.end());
+            for (int t = 0; t < k; ++t) {
+                ja[static_cast<size_t>(q) * k + t] = cand[t].second;
+                if (d2out) d2out[static_cast<size_t>(q) * k + t] = cand[t].first;
+            }
+        }
+    }
+    return 0;
+}
+
+// Squared distances of a stencil table, in the same arithmetic as
+// orc_knn_brute; used to compare stencils up to tie order.
+void orc_stencil_d2(int n, const double* x, const double* y, int k, const int* ja, double Lx,
+                    double Ly, double* d2) {
+#pragma omp parallel for schedule(static)
+    for (int s = 0; s < n; ++s)
+        for (int t = 0; t < k; ++t) {
+            const int j = ja[static_cast<size_t>(s) * k + t];
+            double dx = x[s] - x[j];
+            double dy = y[s] - y[j];
+            if (Lx > 0) {
+                const double hb = 0.5 * Lx;
+                if (dx < -hb) dx = Lx + dx;
+                else if (dx > hb) dx = dx - Lx;
+            }
+            if (Ly > 0) {
+                const double hb = 0.5 * Ly;
+                if (dy < -hb) dy = Ly + dy;
+                else if (dy > hb) dy = dy - Ly;
+            }
+            d2[static_cast<size_t>(s) * k + t] = dx * dx + dy * dy;
+        }
+}
+
+}  // extern "C"

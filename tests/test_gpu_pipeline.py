@@ -1,0 +1,100 @@
+"""End-to-end host call, the uneven (CSR, bucketed) batch and the autotuner,
+each against the oracle or against the fixed-width device path."""
+import numpy as np
+import pytest
+
+import oracle as O
+import rbf_b200 as R
+from conftest import golden
+from rbf_b200 import nodesets as NS
+
+pytestmark = pytest.mark.gpu
+
+
+def test_host_pipeline_equals_device_path(ctx, torch_cuda):
+    T = torch_cuda
+    g = golden("square69_k21")
+    x, y = g["x"], g["y"]
+    n, k = x.size, 21
+    for prec in (R.FP64, R.FP32_IR):
+        d = R.make_desc(2, precision=prec)
+        vals_h = [np.empty(n * k) for _ in range(3)]
+        ja_out = np.empty(n * k, np.int32)
+        info = np.empty(n, np.int32)
+        st = ctx.assemble_host(d, x, y, k, vals_h, ja_out_h=ja_out, info_h=info)
+        np.testing.assert_array_equal(ja_out, g["ja_nanoflann"])
+        assert (info == 0).all() and st["stencils"] == n
+        Wo, _ = O.assemble(x, y, g["ja_nanoflann"], k, 2)
+        tol = 1e-12 if prec == R.FP64 else 1e-10
+        assert O.max_rel_err(np.stack(vals_h), Wo, k).max() <= tol
+
+
+def test_host_pipeline_given_stencils_many_chunks(ctx, torch_cuda):
+    # 300 x 300 periodic grid: several chunks, k=35 degree 3, given stencils
+    x, y, _ = NS.jittered_grid(300, 0.3, seed=21, periodic=True)
+    n, k = x.size, 35
+    T = torch_cuda
+    ja = T.empty(n * k, dtype=T.int32, device="cuda")
+    ctx.knn_stencils(T.as_tensor(x).cuda(), T.as_tensor(y).cuda(), k, ja, period=(1.0, 1.0))
+    ja_h = ja.cpu().numpy()
+    d = R.make_desc(3, precision=R.FP32_IR, period=(1.0, 1.0))
+    vals_h = [np.empty(n * k) for _ in range(3)]
+    ctx.assemble_host(d, x, y, k, vals_h, ja_h=ja_h)
+    rows = np.arange(0, n, 997)
+    idx = (rows[:, None] * k + np.arange(k)[None, :]).ravel()
+    Wo, _ = O.assemble(x, y, ja_h, k, 3, period=(1.0, 1.0))
+    W = np.stack(vals_h)
+    assert O.max_rel_err(W[:, idx], Wo[:, idx], k).max() <= 1e-10
+
+
+def test_csr_uneven_matches_oracle(ctx, torch_cuda):
+    T = torch_cuda
+    # small disk: boundary nodes k in [22, 35] degree 3, interior k in {21, 28, 35}
+    c = NS.config_disk_uneven(n=6000, nb=200, seed=13)
+    kvec = np.minimum(c["kvec"], 35)
+    deg = c["degree"].copy()
+    deg[deg == 4] = 3
+    x, y = c["x"], c["y"]
+    n = x.size
+    kmax = int(kvec.max())
+    jaf = O.knn_brute(x, y, kmax).reshape(n, kmax)
+    ia = np.zeros(n + 1, np.int32)
+    ia[1:] = np.cumsum(kvec)
+    ja = np.concatenate([jaf[s, : kvec[s]] for s in range(n)]).astype(np.int32)
+    for prec, tol in ((R.FP64, 1e-12), (R.FP32_IR, 1e-10)):
+        d = R.make_desc(2, precision=prec)
+        vals = [T.empty(int(ia[-1]), dtype=T.float64, device="cuda") for _ in range(3)]
+        info = T.full((n,), -3, dtype=T.int32, device="cuda")
+        st = ctx.assemble_csr(d, T.as_tensor(x).cuda(), T.as_tensor(y).cuda(),
+                              T.as_tensor(ia).cuda(), T.as_tensor(ja).cuda(), vals,
+                              degree=T.as_tensor(deg).cuda(), info=info, stats=True)
+        T.cuda.synchronize()
+        assert (info.cpu().numpy() == 0).all()
+        assert st["buckets"] >= 2
+        Wo, io = O.assemble_csr(x, y, ia, ja, degree=deg, P=2, Q=0)
+        W = np.stack([v.cpu().numpy() for v in vals])
+        # ragged error per stencil
+        worst = 0.0
+        for s in range(n):
+            a, b = ia[s], ia[s + 1]
+            e = np.abs(W[:, a:b] - Wo[:, a:b]).max(axis=1) / np.abs(Wo[:, a:b]).max(axis=1)
+            worst = max(worst, float(e.max()))
+        assert worst <= tol, (prec, worst)
+
+
+def test_autotune_picks_a_compiled_shape(ctx, torch_cuda):
+    T = torch_cuda
+    g = golden("square69_k21")
+    n, k = g["x"].size, 21
+    d = R.make_desc(2, precision=R.FP32_IR)
+    vals = [T.empty(n * k, dtype=T.float64, device="cuda") for _ in range(3)]
+    v = ctx.autotune(d, T.as_tensor(g["x"]).cuda(), T.as_tensor(g["y"]).cuda(), k,
+                     T.as_tensor(g["ja_nanoflann"]).cuda(), vals)
+    assert v >= 0
+    # the tuned shape is used and still correct
+    info = T.zeros(n, dtype=T.int32, device="cuda")
+    ctx.assemble(d, T.as_tensor(g["x"]).cuda(), T.as_tensor(g["y"]).cuda(), k,
+                 T.as_tensor(g["ja_nanoflann"]).cuda(), vals, info)
+    T.cuda.synchronize()
+    Wo, _ = O.assemble(g["x"], g["y"], g["ja_nanoflann"], k, 2)
+    assert O.max_rel_err(np.stack([v.cpu().numpy() for v in vals]), Wo, k).max() <= 1e-10

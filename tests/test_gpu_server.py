@@ -1,0 +1,71 @@
+"""Continuous-batching server: results are the same alone and in the mix,
+requests beyond the HBM budget are refused, waits are bounded."""
+import time
+
+import numpy as np
+import pytest
+
+import rbf_b200 as R
+from rbf_b200 import nodesets as NS
+
+pytestmark = pytest.mark.gpu
+
+
+def requests():
+    out = []
+    for i, (m, k, P, geo) in enumerate([(40, 21, 2, "square"), (70, 35, 3, "square"),
+                                        (55, 21, 2, "disk"), (90, 35, 3, "square"),
+                                        (30, 21, 2, "disk"), (60, 35, 3, "disk")]):
+        req = dict(n=m * m, geometry=geo, k=k, P=P, Q=2 * P - 1, seed=100 + i)
+        x, y = NS.request_nodes(req)
+        out.append((x, y, k, P))
+    return out
+
+
+def run_alone(x, y, k, P, prec):
+    """The same request through a fresh context, nothing else on the device."""
+    n = x.size
+    d = R.make_desc(P, precision=prec)
+    vals = [np.empty(n * k) for _ in range(3)]
+    ja = np.empty(n * k, np.int32)
+    with R.Context(0) as c:
+        c.assemble_host(d, x, y, k, vals, ja_out_h=ja)
+    return ja, vals
+
+
+def test_same_alone_and_in_the_mix(torch_cuda):
+    reqs = requests()
+    for prec in (R.FP64, R.FP32_IR):
+        srv = R.Server(0, hbm_budget=2 << 30, max_slots=4)
+        try:
+            tickets = [srv.submit(x, y, k, R.make_desc(P, precision=prec)) for x, y, k, P in reqs]
+            for t, (x, y, k, P) in zip(tickets, reqs):
+                st, res = srv.poll(t, wait_ms=60000)
+                assert st == 0 and res.status == 0 and res.singular == 0
+                vals, ja = srv.fetch(t, x.size, k, 3, with_ja=True)
+                ja1, vals1 = run_alone(x, y, k, P, prec)
+                np.testing.assert_array_equal(ja, ja1)
+                for a, b in zip(vals, vals1):
+                    np.testing.assert_array_equal(a, b)  # bit-identical
+                assert res.end_ms >= res.start_ms >= res.submit_ms
+                assert srv.release(t) == 0
+            assert srv.resident_bytes() == 0
+        finally:
+            srv.close()
+
+
+def test_budget_and_bounded_waits(torch_cuda):
+    srv = R.Server(0, hbm_budget=1 << 20, max_slots=2)  # 1 MiB
+    try:
+        x, y, _ = NS.jittered_grid(200, 0.3, seed=1)
+        with pytest.raises(R.RbfError) as e:
+            srv.submit(x, y, 21, R.make_desc(2))
+        assert e.value.status == R.EBUDGET
+        x, y, _ = NS.jittered_grid(20, 0.3, seed=1)
+        t = srv.submit(x, y, 21, R.make_desc(2))
+        st, _ = srv.poll(t, wait_ms=30000)
+        assert st == 0
+        assert srv.poll(t + 999, wait_ms=0)[0] == R.ENOTFOUND
+        assert srv.release(t) == 0
+    finally:
+        srv.close()
