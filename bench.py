@@ -255,6 +255,13 @@ def main():
     d_mix = R.make_desc(P, Q, R.DEFAULT_OPS, R.FP32_IR, True, period=per)
     d_f64 = R.make_desc(P, Q, R.DEFAULT_OPS, R.FP64, True, period=per)
 
+    # project autotuner: kernel shape and CTAs per SM for both precisions
+    ctx.knn_stencils(xd, yd, K, ja, period=per, stream=stream)
+    tuned = {}
+    for nm, dsc in (("mixed", d_mix), ("fp64", d_f64)):
+        v = ctx.autotune(dsc, xd, yd, K, ja, vals)
+        tuned[nm] = R.variant_name(v)
+
     def step(desc, stats=False):
         ctx.knn_stencils(xd, yd, K, ja, period=per, stream=stream)
         return ctx.assemble(desc, xd, yd, K, ja, vals, info, stats=stats, stream=stream)
@@ -389,6 +396,7 @@ def main():
                 "d2h_bytes_per_step": nk * (8 * NRHS + 4),
                 "device_ms": e2e_dev_ms / e2e_steps},
         "gpu_launches": launches,
+        "kernel_shapes": tuned,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
                      "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                      "traffic": traffic_per_launch(),

@@ -46,6 +46,7 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 
 #include "asm_math.cuh"
 
@@ -104,7 +105,9 @@ struct AsmCfg {
     static constexpr int KPL = (KMAX + G - 1) / G;       // gathered nodes per lane
     static constexpr int VEC = 16 / sizeof(T);
     static_assert(CW % VEC == 0, "register columns must tile the vector width");
-    static constexpr int BW = ((NTP + NRHS + VEC - 1) / VEC) * VEC;  // pivot row buffer
+    static_assert(NTP <= 128, "pivot keys carry the row index in 7 bits");
+    // pivot row buffer: NTP columns, NRHS right-hand sides, the pivot's reciprocal
+    static constexpr int BW = ((NTP + NRHS + 1 + VEC - 1) / VEC) * VEC;
     static constexpr int LDS = NTP;                                   // S row stride
     static constexpr int al16(int b) { return (b + 15) & ~15; }
     static constexpr int off_cx = 0;
@@ -116,10 +119,28 @@ struct AsmCfg {
     static constexpr int off_pm = off_phi + (MIXED ? al16(8 * NPAIR) : 0);
     static constexpr int off_x64 = off_pm + (MIXED ? al16(8 * KMAX * NP) : 0);
     static constexpr int off_b64 = off_x64 + (MIXED ? al16(8 * NTP * NRHS) : 0);
-    static constexpr int bytes = off_b64 + (MIXED ? al16(8 * NTP * NRHS) : 0);
+    static constexpr int off_piv = off_b64 + (MIXED ? al16(8 * NTP * NRHS) : 0);
+    static constexpr int bytes = off_piv + al16(4 * NTP);  // row pivoted at each step
     // S position of column c (de-interleaved by lane-column)
     static __device__ __forceinline__ int scol(int c) { return (c % GC) * CW + c / GC; }
 };
+
+// Register rows are kept as 16-byte tuples (float4 / double2) so the pivot
+// row goes to shared memory straight from aligned register quads.
+template <typename T>
+struct Vec;
+template <>
+struct Vec<float> {
+    using type = float4;
+};
+template <>
+struct Vec<double> {
+    using type = double2;
+};
+__device__ __forceinline__ float& comp(float4& v, int t) {
+    return t == 0 ? v.x : (t == 1 ? v.y : (t == 2 ? v.z : v.w));
+}
+__device__ __forceinline__ double& comp(double2& v, int t) { return t == 0 ? v.x : v.y; }
 
 // Packed index of the pair (i, j), i < j, of a k-node stencil.
 __device__ __forceinline__ int tri(int i, int j, int k) {
@@ -129,16 +150,35 @@ __device__ __forceinline__ double phi_at(const double* phi, int i, int j, int k)
     return i == j ? 0.0 : (i < j ? phi[tri(i, j, k)] : phi[tri(j, i, k)]);
 }
 
-// Right-hand side q for node row (xi, yi) and for polynomial row m, FP64.
-template <int P, int Q>
-__device__ __forceinline__ double rhs_node(const AsmParams& p, int q, double xi, double yi, int e) {
-    const int op = p.col_op[q];
-    if (op == kOpInterp) {
-        const double xe = scalbn(p.xc[p.col_ic[q]], -e);
-        const double ye = scalbn(p.yc[p.col_ic[q]], -e);
-        return phs64<Q>(dist2(dsub(xe, xi), dsub(ye, yi)));
+// Right-hand sides of node row (xi, yi): every column q < nrhs, FP64, the
+// PHS power r^(Q-2) shared by the derivative operators (one square root).
+template <int P, int Q, int NRHS>
+__device__ __forceinline__ void rhs_node(const AsmParams& p, double xi, double yi, int e,
+                                         double* out) {
+    const double r2 = dist2(xi, yi);
+    const double rq2 = phs64<Q - 2>(r2);
+    const double q = static_cast<double>(Q);
+    const double qr = dmul(q, rq2);
+#pragma unroll
+    for (int c = 0; c < NRHS; ++c) {
+        double v = 0.0;
+        if (c < p.nrhs) {
+            const int op = p.col_op[c];
+            switch (op) {
+                case kOpInterp: {
+                    const double xe = scalbn(p.xc[p.col_ic[c]], -e);
+                    const double ye = scalbn(p.yc[p.col_ic[c]], -e);
+                    v = phs64<Q>(dist2(dsub(xe, xi), dsub(ye, yi)));
+                    break;
+                }
+                case kOpLaplace: v = dmul(q * q, rq2); break;
+                case kOpDx: v = -dmul(qr, xi); break;
+                case kOpDy: v = -dmul(qr, yi); break;
+                default: v = phs_op_origin<Q>(op, xi, yi); break;
+            }
+        }
+        out[c] = v;
     }
-    return phs_op_origin<Q>(op, xi, yi);
 }
 template <int P>
 __device__ __forceinline__ double rhs_poly(const AsmParams& p, int q, int m, int e) {
@@ -205,14 +245,27 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, char* sm
     __syncwarp(gmask);
 
     // ---- fill the staging matrix S (permuted, padded) and the right-hand sides
-    // phi block: each unordered pair once
-    for (int i = 0; i < ks - 1; ++i) {
-        const double xi = cx[i], yi = cy[i];
-        for (int j = i + 1 + lg; j < ks; j += G) {
-            const double v = phs64<Q>(dist2(dsub(cx[j], xi), dsub(cy[j], yi)));
+    // phi block: each unordered pair once. The pairs (i < j) are walked as
+    // one flat sequence, G at a time: every lane busy, iterations independent.
+    {
+        const int npair = ks * (ks - 1) / 2;
+        // (i, j) of pair number lg; past the end of row i (j >= ks) the walk
+        // continues in row i + 1 at j - ks + i + 2
+        int i = 0, j = 1 + lg;
+        while (i < ks - 1 && j >= ks) {
+            j += i + 2 - ks;
+            ++i;
+        }
+        for (int t = lg; t < npair; t += G) {
+            const double v = phs64<Q>(dist2(dsub(cx[j], cx[i]), dsub(cy[j], cy[i])));
             S[(NP + i) * LDS + C::scol(NP + j)] = static_cast<T>(v);
             S[(NP + j) * LDS + C::scol(NP + i)] = static_cast<T>(v);
-            if constexpr (MIXED) phi[tri(i, j, ks)] = v;
+            if constexpr (MIXED) phi[t] = v;  // t = tri(i, j, ks)
+            j += G;
+            while (i < ks - 1 && j >= ks) {
+                j += i + 2 - ks;
+                ++i;
+            }
         }
     }
     // everything else, one row per lane
@@ -241,11 +294,12 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, char* sm
             }
             Sr[C::scol(r)] = T(0);
             for (int c = n; c < NTP; ++c) Sr[C::scol(c)] = T(0);
+            double rv[NRHS];
+            rhs_node<P, Q, NRHS>(p, xi, yi, e, rv);
 #pragma unroll
             for (int q = 0; q < NRHS; ++q) {
-                const double v = q < p.nrhs ? rhs_node<P, Q>(p, q, xi, yi, e) : 0.0;
-                X[r * NRHS + q] = static_cast<T>(v);
-                if constexpr (MIXED) b64[r * NRHS + q] = v;
+                X[r * NRHS + q] = static_cast<T>(rv[q]);
+                if constexpr (MIXED) b64[r * NRHS + q] = rv[q];
             }
         } else {
             for (int c = 0; c < NTP; ++c) Sr[C::scol(c)] = (c == r) ? T(1) : T(0);
@@ -259,24 +313,19 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, char* sm
     __syncwarp(gmask);
 
     // ---- rows into registers (vector loads)
-    T a[R][CW];
+    using V = typename Vec<T>::type;
+    constexpr int NV = CW / VEC;  // register tuples per row slot
+    V a[R][NV];
     T yv[R][NRHS];
     int pst[R];
     T dinv[R];
+    int* pivrow = reinterpret_cast<int*>(smem + C::off_piv);
 #pragma unroll
     for (int sl = 0; sl < R; ++sl) {
         const int r = lr + GR * sl;
-        const T* Sr = S + r * LDS + lc * CW;
+        const V* Sr = reinterpret_cast<const V*>(S + r * LDS + lc * CW);
 #pragma unroll
-        for (int cl = 0; cl < CW; cl += VEC) {
-            if constexpr (VEC == 4) {
-                const float4 v = *reinterpret_cast<const float4*>(Sr + cl);
-                a[sl][cl] = v.x; a[sl][cl + 1] = v.y; a[sl][cl + 2] = v.z; a[sl][cl + 3] = v.w;
-            } else {
-                const double2 v = *reinterpret_cast<const double2*>(Sr + cl);
-                a[sl][cl] = v.x; a[sl][cl + 1] = v.y;
-            }
-        }
+        for (int cb = 0; cb < NV; ++cb) a[sl][cb] = Sr[cb];
 #pragma unroll
         for (int q = 0; q < NRHS; ++q) yv[sl][q] = X[r * NRHS + q];
         pst[sl] = kFree;
@@ -284,168 +333,186 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, char* sm
     }
 
     // ---- elimination with row-implicit partial pivoting
+    //
+    // A runtime loop over blocks of SB = GC * VEC steps keeps the code small
+    // enough for the instruction cache. The steps of a block pivot on the
+    // columns held in register tuple 0 (static components); after the block,
+    // tuple 0 -- now final: L multipliers of the rows not yet pivoted and U
+    // entries of the others -- goes to S (physical row layout), and the
+    // remaining tuples shift down by one. The blocks run in NWC width classes:
+    // class w updates the NV - w*NV/NWC tuples still active at its start
+    // (tuples that died inside the class hold zeros), so the bodies compiled
+    // are NWC, not NTP.
+    constexpr int SB = GC * VEC;
+    static_assert(NTP % SB == 0, "padded size must be a whole number of blocks");
+    constexpr int NWC = NV >= 4 ? 4 : NV;
     int info = 0;
+    auto step_block = [&](auto width, int b) {
+        constexpr int W = decltype(width)::value;
 #pragma unroll
-    for (int c = 0; c < NTP; ++c) {
-        const int lcc = c % GC, clc = c / GC;
-        T* B = buf + (c & 1) * BW;
-        // 1. pivot search
-        int prow;
-        bool zero_pivot;
-        if constexpr (sizeof(T) == 4) {
-            uint32_t best = 0;
-            if (lc == lcc) {
+        for (int j = 0; j < SB; ++j) {
+            const int c = b * SB + j;
+            const int lcc = j % GC, ctc = j / GC;  // lane-column and component of column c
+            T* B = buf + (j & 1) * BW;
+            // 1. pivot search. The pivot is the unused row of largest |a(r, c)|
+            // compared without the 7 lowest bits of its binary representation,
+            // ties to the lowest row (the oracle's rule); the row index rides in
+            // those 7 bits, so one max-reduction (FP32) or two (FP64: high word,
+            // then low word | row) finds it. Used rows send 0.
+            int prow;
+            bool zero_pivot;
+            T my_inv, lbest = T(1);
+            if constexpr (sizeof(T) == 4) {
+                uint32_t best = 0;
 #pragma unroll
                 for (int sl = 0; sl < R; ++sl) {
                     const uint32_t kk =
-                        (pst[sl] == kFree) ? __float_as_uint(fabsf(a[sl][clc])) + 1u : 0u;
-                    best = max(best, kk);
+                        (lc == lcc && pst[sl] == kFree)
+                            ? ((((__float_as_uint(fabsf(comp(a[sl][0], ctc))) >> 7) + 1u) << 7) |
+                               (uint32_t)(127 - (lr + GR * sl)))
+                            : 0u;
+                    if (kk > best) {
+                        best = kk;
+                        lbest = comp(a[sl][0], ctc);
+                    }
                 }
-            }
-            const uint32_t m = __reduce_max_sync(gmask, best);
-            uint32_t cand = 0xffffffffu;
-            if (lc == lcc) {
-#pragma unroll
-                for (int sl = R - 1; sl >= 0; --sl) {
-                    const uint32_t kk =
-                        (pst[sl] == kFree) ? __float_as_uint(fabsf(a[sl][clc])) + 1u : 0u;
-                    if (kk == m) cand = (uint32_t)(lr + GR * sl);
-                }
-            }
-            prow = (int)__reduce_min_sync(gmask, cand);
-            zero_pivot = (m <= 1u);
-        } else {
-            unsigned long long best = 0;
-            if (lc == lcc) {
+                // this lane's best candidate's reciprocal, while the group
+                // reduces: if this lane owns the pivot, it is the pivot's
+                my_inv = __frcp_rn(lbest);
+                const uint32_t m = __reduce_max_sync(gmask, best);
+                prow = 127 - (int)(m & 127u);
+                zero_pivot = (m >> 7) <= 1u;
+            } else {
+                uint32_t bhi = 0, blo = 0;
 #pragma unroll
                 for (int sl = 0; sl < R; ++sl) {
-                    const unsigned long long kk =
-                        (pst[sl] == kFree)
-                            ? (unsigned long long)__double_as_longlong(fabs((double)a[sl][clc])) + 1ull
-                            : 0ull;
-                    best = best > kk ? best : kk;
+                    const unsigned long long bits =
+                        (unsigned long long)__double_as_longlong(fabs((double)comp(a[sl][0], ctc)));
+                    const bool ok = lc == lcc && pst[sl] == kFree;
+                    const uint32_t hi = ok ? (uint32_t)(bits >> 32) + 1u : 0u;
+                    const uint32_t lo = ok ? ((((uint32_t)bits) >> 7) << 7) |
+                                                 (uint32_t)(127 - (lr + GR * sl))
+                                           : 0u;
+                    if (hi > bhi || (hi == bhi && lo > blo)) {
+                        bhi = hi;
+                        blo = lo;
+                        lbest = comp(a[sl][0], ctc);
+                    }
                 }
+                my_inv = __drcp_rn(lbest);  // = the oracle's 1.0 / pivot (both rounded once)
+                const uint32_t mh = __reduce_max_sync(gmask, bhi);
+                const uint32_t ml = __reduce_max_sync(gmask, bhi == mh ? blo : 0u);
+                prow = 127 - (int)(ml & 127u);
+                zero_pivot = mh <= 1u && (ml >> 7) == 0u;
             }
-            const uint32_t mh = __reduce_max_sync(gmask, (uint32_t)(best >> 32));
-            const uint32_t ml =
-                __reduce_max_sync(gmask, ((uint32_t)(best >> 32) == mh) ? (uint32_t)best : 0u);
-            const unsigned long long m = ((unsigned long long)mh << 32) | ml;
-            uint32_t cand = 0xffffffffu;
-            if (lc == lcc) {
-#pragma unroll
-                for (int sl = R - 1; sl >= 0; --sl) {
-                    const unsigned long long kk =
-                        (pst[sl] == kFree)
-                            ? (unsigned long long)__double_as_longlong(fabs((double)a[sl][clc])) + 1ull
-                            : 0ull;
-                    if (kk == m) cand = (uint32_t)(lr + GR * sl);
-                }
-            }
-            prow = (int)__reduce_min_sync(gmask, cand);
-            zero_pivot = (m <= 1ull);
-        }
-        if (zero_pivot && info == 0) info = c + 1;
-        const int plr = prow % GR, psl = prow / GR;
+            if (zero_pivot && info == 0) info = c + 1;
+            const int plr = prow % GR, psl = prow / GR;
+            if (lg == 0) pivrow[c] = prow;
 
-        // 2. pivot row to shared memory (owner lane-row), then broadcast
-        if (lr == plr) {
+            // 2. pivot row to shared memory (owner lane-row), then broadcast
+            if (lr == plr) {
+#pragma unroll
+                for (int sl = 0; sl < R; ++sl) {
+                    if (sl == psl) {
+                        V* Bv = reinterpret_cast<V*>(B + lc * CW);
+#pragma unroll
+                        for (int cb = 0; cb < W; ++cb) Bv[cb] = a[sl][cb];
+                        if (lc == 0) {
+#pragma unroll
+                            for (int q = 0; q < NRHS; ++q) B[NTP + q] = yv[sl][q];
+                        }
+                        if (lc == lcc) B[BW - 1] = my_inv;
+                        pst[sl] = c;
+                    }
+                }
+            }
+            __syncwarp(gmask);
+            const T inv = B[BW - 1];
+            if (lr == plr) {
+#pragma unroll
+                for (int sl = 0; sl < R; ++sl)
+                    if (sl == psl) dinv[sl] = inv;
+            }
+            // 3. multipliers (kept as the L factor) and the update
+            T l[R];
 #pragma unroll
             for (int sl = 0; sl < R; ++sl) {
-                if (sl == psl) {
+                T av = comp(a[sl][0], ctc);
+                if constexpr (GC > 1) av = __shfl_sync(gmask, av, lr * GC + lcc, G);
+                l[sl] = (pst[sl] == kFree) ? av * inv : T(0);
+                if (lc == lcc && pst[sl] == kFree) comp(a[sl][0], ctc) = l[sl];
+            }
+            const V* Bv = reinterpret_cast<const V*>(B + lc * CW);
 #pragma unroll
-                    for (int cl = (clc / VEC) * VEC; cl < CW; cl += VEC) {
-                        if constexpr (VEC == 4) {
-                            *reinterpret_cast<float4*>(B + lc * CW + cl) = make_float4(
-                                a[sl][cl], a[sl][cl + 1], a[sl][cl + 2], a[sl][cl + 3]);
-                        } else {
-                            *reinterpret_cast<double2*>(B + lc * CW + cl) =
-                                make_double2(a[sl][cl], a[sl][cl + 1]);
-                        }
-                    }
-                    if (lc == 0) {
+            for (int cb = 0; cb < W; ++cb) {
+                V u = Bv[cb];
 #pragma unroll
-                        for (int q = 0; q < NRHS; ++q) B[NTP + q] = yv[sl][q];
+                for (int t = 0; t < VEC; ++t) {
+                    if (cb == 0 && t < ctc) continue;  // columns already eliminated
+                    if (cb == 0 && t == ctc) {
+                        if constexpr (GC == 1) continue;
+                        if (lc <= lcc) continue;       // column c itself or before it
                     }
-                    pst[sl] = c;
+#pragma unroll
+                    for (int sl = 0; sl < R; ++sl)
+                        comp(a[sl][cb], t) = fma(-l[sl], comp(u, t), comp(a[sl][cb], t));
                 }
             }
-        }
-        __syncwarp(gmask);
-        const T inv = T(1) / B[lcc * CW + clc];
-        if (lr == plr) {
 #pragma unroll
-            for (int sl = 0; sl < R; ++sl)
-                if (sl == psl) dinv[sl] = inv;
+            for (int q = 0; q < NRHS; ++q) {
+                const T uq = B[NTP + q];
+#pragma unroll
+                for (int sl = 0; sl < R; ++sl) yv[sl][q] = fma(-l[sl], uq, yv[sl][q]);
+            }
         }
-        // 3. multipliers (kept as the L factor) and the update
-        T l[R];
+        // tuple 0 is final: to S at its tuple position, then shift down
 #pragma unroll
         for (int sl = 0; sl < R; ++sl) {
-            T av = a[sl][clc];
-            if constexpr (GC > 1) av = __shfl_sync(gmask, av, lr * GC + lcc, G);
-            l[sl] = (pst[sl] == kFree) ? av * inv : T(0);
-            if (lc == lcc && pst[sl] == kFree) a[sl][clc] = l[sl];
+            reinterpret_cast<V*>(S + (lr + GR * sl) * LDS + lc * CW)[b] = a[sl][0];
+#pragma unroll
+            for (int cb = 0; cb + 1 < W; ++cb) a[sl][cb] = a[sl][cb + 1];
+            a[sl][W - 1] = V{};
         }
-#pragma unroll
-        for (int cb = (clc / VEC) * VEC; cb < CW; cb += VEC) {
-            T u[VEC];
-            if constexpr (VEC == 4) {
-                const float4 v4 = *reinterpret_cast<const float4*>(B + lc * CW + cb);
-                u[0] = v4.x; u[1] = v4.y; u[2] = v4.z; u[3] = v4.w;
-            } else {
-                const double2 v2 = *reinterpret_cast<const double2*>(B + lc * CW + cb);
-                u[0] = v2.x; u[1] = v2.y;
-            }
-#pragma unroll
-            for (int t = 0; t < VEC; ++t) {
-                const int cl = cb + t;
-                if (cl < clc) continue;
-                if (cl == clc) {
-                    if constexpr (GC == 1) continue;
-                    if (lc <= lcc) continue;
-                }
-#pragma unroll
-                for (int sl = 0; sl < R; ++sl) a[sl][cl] = fma(-l[sl], u[t], a[sl][cl]);
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < NRHS; ++q) {
-            const T uq = B[NTP + q];
-#pragma unroll
-            for (int sl = 0; sl < R; ++sl) yv[sl][q] = fma(-l[sl], uq, yv[sl][q]);
-        }
-    }
-
-    // ---- factors back to S (physical row layout); the registers die here
-#pragma unroll
-    for (int sl = 0; sl < R; ++sl) {
-        T* Sr = S + (lr + GR * sl) * LDS + lc * CW;
-#pragma unroll
-        for (int cl = 0; cl < CW; cl += VEC) {
-            if constexpr (VEC == 4) {
-                *reinterpret_cast<float4*>(Sr + cl) =
-                    make_float4(a[sl][cl], a[sl][cl + 1], a[sl][cl + 2], a[sl][cl + 3]);
-            } else {
-                *reinterpret_cast<double2*>(Sr + cl) = make_double2(a[sl][cl], a[sl][cl + 1]);
-            }
-        }
+    };
+    {
+        int b = 0;
+        auto run_class = [&](auto wc) {
+            constexpr int w = decltype(wc)::value;
+            constexpr int W = NV - (w * NV) / NWC;  // active tuples at the class start
+            constexpr int bend = ((w + 1) * NV) / NWC;
+#pragma unroll 1
+            for (; b < bend; ++b) step_block(std::integral_constant<int, W>{}, b);
+        };
+        run_class(std::integral_constant<int, 0>{});
+        if constexpr (NWC > 1) run_class(std::integral_constant<int, 1>{});
+        if constexpr (NWC > 2) run_class(std::integral_constant<int, 2>{});
+        if constexpr (NWC > 3) run_class(std::integral_constant<int, 3>{});
     }
     __syncwarp(gmask);
 
-    // column-oriented back substitution from S into X[c][q]
+    // Column-oriented back substitution from S into X[c][q], a runtime loop:
+    // the owner lane of step c's pivot row forms x_c = y * (1/pivot) and
+    // broadcasts it by shuffle; rows pivoted before c update with S(r, c).
     auto back_substitute = [&](T (&yy)[R][NRHS]) {
 #pragma unroll 1
         for (int c = NTP - 1; c >= 0; --c) {
-#pragma unroll
-            for (int sl = 0; sl < R; ++sl)
-                if (pst[sl] == c && lc == 0) {
-#pragma unroll
-                    for (int q = 0; q < NRHS; ++q) X[c * NRHS + q] = yy[sl][q] * dinv[sl];
-                }
-            __syncwarp(gmask);
+            const int pr = pivrow[c];
+            const int osl = pr / GR, olane = (pr % GR) * GC;
             T xq[NRHS];
+            T dv = dinv[0];
 #pragma unroll
-            for (int q = 0; q < NRHS; ++q) xq[q] = X[c * NRHS + q];
+            for (int sl = 1; sl < R; ++sl) dv = (osl == sl) ? dinv[sl] : dv;
+#pragma unroll
+            for (int q = 0; q < NRHS; ++q) {
+                T v = yy[0][q];
+#pragma unroll
+                for (int sl = 1; sl < R; ++sl) v = (osl == sl) ? yy[sl][q] : v;
+                xq[q] = __shfl_sync(gmask, v * dv, olane, G);
+            }
+            if (lg == 0) {
+#pragma unroll
+                for (int q = 0; q < NRHS; ++q) X[c * NRHS + q] = xq[q];
+            }
             const int sc = C::scol(c);
 #pragma unroll
             for (int sl = 0; sl < R; ++sl) {
@@ -505,8 +572,19 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, char* sm
 #pragma unroll
                         for (int q = 0; q < NRHS; ++q) acc[q] = fma(-mv, x64[m * NRHS + q], acc[q]);
                     }
-                    for (int j = 0; j < ks; ++j) {
-                        const double fv = phi_at(phi, i, j, ks);
+                    // phi(i, j) for j < i: column i of the packed upper triangle,
+                    // tri(j, i) advancing by ks - j - 2; for j > i: row i, contiguous
+                    int t = i - 1;  // tri(0, i)
+                    for (int j = 0; j < i; ++j) {
+                        const double fv = phi[t];
+                        t += ks - j - 2;
+#pragma unroll
+                        for (int q = 0; q < NRHS; ++q)
+                            acc[q] = fma(-fv, x64[(NP + j) * NRHS + q], acc[q]);
+                    }
+                    const double* prow_i = phi + (i < ks - 1 ? tri(i, i + 1, ks) : 0);
+                    for (int j = i + 1; j < ks; ++j) {
+                        const double fv = prow_i[j - i - 1];
 #pragma unroll
                         for (int q = 0; q < NRHS; ++q)
                             acc[q] = fma(-fv, x64[(NP + j) * NRHS + q], acc[q]);
@@ -528,17 +606,16 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, char* sm
             __syncwarp(gmask);
 #pragma unroll 1
             for (int t = 0; t < NTP; ++t) {
-                T* Z = buf + (t & 1) * BW;
-#pragma unroll
-                for (int sl = 0; sl < R; ++sl)
-                    if (pst[sl] == t && lc == 0) {
-#pragma unroll
-                        for (int q = 0; q < NRHS; ++q) Z[q] = rv[sl][q];
-                    }
-                __syncwarp(gmask);
+                const int pr = pivrow[t];
+                const int osl = pr / GR, olane = (pr % GR) * GC;
                 T zq[NRHS];
 #pragma unroll
-                for (int q = 0; q < NRHS; ++q) zq[q] = Z[q];
+                for (int q = 0; q < NRHS; ++q) {
+                    T v = rv[0][q];
+#pragma unroll
+                    for (int sl = 1; sl < R; ++sl) v = (osl == sl) ? rv[sl][q] : v;
+                    zq[q] = __shfl_sync(gmask, v, olane, G);
+                }
                 const int st = C::scol(t);
 #pragma unroll
                 for (int sl = 0; sl < R; ++sl) {
@@ -565,9 +642,19 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, char* sm
                 worst = fmaxf(worst, xmax > 0.f ? dmax / xmax : dmax);
             }
             __syncwarp(gmask);
-            if (!(worst == worst)) failed = true;  // NaN
-            else if (worst <= (float)p.ir_tol) converged = true;
-            else if (sweeps >= 2 && worst > 0.5f * prev) failed = true;  // stalled
+            // The correction of sweep k measures the error before it (tau_k);
+            // the error left after it is about tau_k * rho / (1 - rho) with
+            // rho = tau_k / tau_(k-1) the observed contraction. Converged when
+            // that prediction is below tol (or the correction itself is at the
+            // FP64 floor); stalled (rho > 1/2) or NaN -> FP64 fallback.
+            if (!(worst == worst)) {
+                failed = true;
+            } else {
+                const float rho = sweeps >= 2 ? worst / fmaxf(prev, 1e-38f) : 1.0f;
+                const float left = rho < 0.5f ? worst * rho / (1.0f - rho) : worst;
+                if (left <= (float)p.ir_tol || worst <= 1e-15f) converged = true;
+                else if (sweeps >= 2 && rho > 0.5f) failed = true;
+            }
             prev = worst;
         }
         if (lg == 0) {
@@ -604,20 +691,23 @@ __global__ void __launch_bounds__(BLOCK, MINB) asm_kernel(AsmParams p) {
     const unsigned gmask = group_mask(G);
     const int n = p.nitems_dev ? *p.nitems_dev : p.nitems;
     const int* list = (p.list && p.list_off_dev) ? p.list + *p.list_off_dev : p.list;
+    const int ngroups = gridDim.x * GPB;
+    int it = blockIdx.x * GPB + gib;
     if (p.work) {
-        for (;;) {
-            int it = 0;
-            if (lg == 0) it = atomicAdd(p.work, 1);
-            it = __shfl_sync(gmask, it, 0, G);
-            if (it >= n) break;
-            const int s = list ? list[it] : p.item_base + it;
-            assemble_one<T, GR, GC, NTP, NRHS, P, Q, MIXED>(p, s, smem, lg, gmask);
-        }
-    } else {
-        const int ngroups = gridDim.x * GPB;
-        for (int it = blockIdx.x * GPB + gib; it < n; it += ngroups) {
-            const int s = list ? list[it] : p.item_base + it;
-            assemble_one<T, GR, GC, NTP, NRHS, P, Q, MIXED>(p, s, smem, lg, gmask);
+        int v = 0;
+        if (lg == 0) v = atomicAdd(p.work, 1);
+        it = __shfl_sync(gmask, v, 0, G);
+    }
+    // one call site: the stencil body is inlined once
+    while (it < n) {
+        const int s = list ? list[it] : p.item_base + it;
+        assemble_one<T, GR, GC, NTP, NRHS, P, Q, MIXED>(p, s, smem, lg, gmask);
+        if (p.work) {
+            int v = 0;
+            if (lg == 0) v = atomicAdd(p.work, 1);
+            it = __shfl_sync(gmask, v, 0, G);
+        } else {
+            it += ngroups;
         }
     }
 }

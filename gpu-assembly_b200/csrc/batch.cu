@@ -179,7 +179,7 @@ int rbfb_assemble_csr(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const
     p.scale = desc->scale;
     p.info = info;
     p.max_sweeps = desc->max_sweeps > 0 ? desc->max_sweeps : 6;
-    p.ir_tol = desc->ir_tol > 0 ? desc->ir_tol : 1e-13;
+    p.ir_tol = desc->ir_tol > 0 ? desc->ir_tol : 1e-11;
     p.list = b->list;
 
     cudaEvent_t e0 = nullptr, e1 = nullptr;

@@ -257,7 +257,10 @@ __global__ void __launch_bounds__(kWarps * 32) query_kernel(QueryArgs a) {
         }
         bool done = false;
         for (int attempt = 0; attempt < 64 && !done; ++attempt) {
-            const int Rx = min(R, (g.cx - 1) / 2 + 1), Ry = min(R, (g.cy - 1) / 2 + 1);
+            // periodic axes: never more than one period (no cell twice); open
+            // axes: up to the whole grid (the clamp below keeps it in range)
+            const int Rx = g.Lx > 0 ? min(R, (g.cx - 1) / 2 + 1) : min(R, g.cx);
+            const int Ry = g.Ly > 0 ? min(R, (g.cy - 1) / 2 + 1) : min(R, g.cy);
             const bool fullx = g.Lx > 0 ? (2 * Rx + 1 >= g.cx) : false;
             const bool fully = g.Ly > 0 ? (2 * Ry + 1 >= g.cy) : false;
             // x/y cell ranges (periodic: wrapped, never more than the grid)

@@ -176,7 +176,7 @@ int base_params(rbfb_ctx* ctx, const rbfb_desc* d, int nstencils, const double* 
     p.scale = d->scale;
     p.info = info;
     p.max_sweeps = d->max_sweeps > 0 ? d->max_sweeps : 6;
-    p.ir_tol = d->ir_tol > 0 ? d->ir_tol : 1e-13;
+    p.ir_tol = d->ir_tol > 0 ? d->ir_tol : 1e-11;
     p.fb_count = &ctr->fb_count;
     p.sweeps_max = &ctr->sweeps_max;
     p.sweeps_sum = &ctr->sweeps_sum;

@@ -11,7 +11,7 @@
 #include <tuple>
 #include <vector>
 
-#include "../../include/rbf_b200.h"
+#include "rbf_b200.h"
 #include "asm_kernel.cuh"
 #include "asm_variants.h"
 

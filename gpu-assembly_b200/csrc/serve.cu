@@ -118,14 +118,10 @@ void CUDART_CB on_done(void* p) {
     delete a;
 }
 
-// Enqueue one request on a slot (called by the worker with the lock held).
+// Enqueue one admitted request on its slot (the worker, without the lock).
 int launch(rbfb_server* s, Slot& sl, Req* r) {
     cudaStream_t st = sl.stream;
-    r->slot = &sl;
     r->stream = st;
-    r->state = State::Running;
-    r->t_start = s->now_ms();
-    sl.busy = r;
     const size_t n = r->n, nk = n * r->k;
     auto alloc = [&](void** p, size_t b) { return cudaMallocAsync(p, b, st); };
     cudaError_t e = cudaSuccess;
@@ -159,36 +155,53 @@ int launch(rbfb_server* s, Slot& sl, Req* r) {
     return e ? RBFB_ECUDA : RBFB_OK;
 }
 
+// The worker admits one request at a time under the lock, then launches it
+// with the lock released: no thread holds the server lock across a CUDA
+// call, so the completion callback (which takes the lock) can never wait on
+// a thread that waits on CUDA.
 void worker_loop(rbfb_server* s) {
     cudaSetDevice(s->device);
-    std::unique_lock<std::mutex> l(s->mu);
-    while (!s->stop) {
-        bool progressed = false;
-        for (auto it = s->queue.begin(); it != s->queue.end();) {
-            Req* r = s->reqs[*it].get();
-            Slot* free_slot = nullptr;
+    for (;;) {
+        Req* r = nullptr;
+        Slot* slot = nullptr;
+        {
+            std::unique_lock<std::mutex> l(s->mu);
+            if (s->stop) return;
             for (auto& sl : s->slots)
                 if (!sl.busy) {
-                    free_slot = &sl;
+                    slot = &sl;
                     break;
                 }
-            if (!free_slot) break;
-            if (s->resident + r->bytes > s->budget) {
-                ++it;  // first fit: a later, smaller request may go ahead
+            if (slot) {
+                for (auto it = s->queue.begin(); it != s->queue.end(); ++it) {
+                    Req* c = s->reqs[*it].get();
+                    if (s->resident + c->bytes > s->budget) continue;  // first fit
+                    r = c;
+                    s->resident += c->bytes;
+                    s->queue.erase(it);
+                    r->state = State::Running;
+                    r->slot = slot;
+                    slot->busy = r;
+                    r->t_start = s->now_ms();
+                    break;
+                }
+            }
+            if (!r) {
+                s->cv.wait_for(l, std::chrono::milliseconds(1));
                 continue;
             }
-            s->resident += r->bytes;
-            it = s->queue.erase(it);
-            const int rc = launch(s, *free_slot, r);
-            if (rc != RBFB_OK) {
+        }
+        const int rc = launch(s, *slot, r);
+        if (rc != RBFB_OK) {
+            {
+                std::lock_guard<std::mutex> l(s->mu);
                 r->status = rc;
                 r->state = State::Failed;
-                free_slot->busy = nullptr;
-                s->done_cv.notify_all();
+                slot->busy = nullptr;
+                r->slot = nullptr;
             }
-            progressed = true;
+            s->done_cv.notify_all();
         }
-        if (!progressed) s->cv.wait_for(l, std::chrono::milliseconds(2));
     }
 }
 
@@ -272,26 +285,32 @@ int rbfb_server_submit(rbfb_server* s, const rbfb_request* req, long long* ticke
 
 int rbfb_server_poll(rbfb_server* s, long long ticket, int wait_ms, rbfb_result* res) {
     if (!s) return RBFB_EINVAL;
-    std::unique_lock<std::mutex> l(s->mu);
-    auto it = s->reqs.find(ticket);
-    if (it == s->reqs.end()) return RBFB_ENOTFOUND;
-    Req* r = it->second.get();
-    auto finished = [&] { return r->state == State::Done || r->state == State::Failed; };
-    if (!finished()) {
-        if (wait_ms == 0) return RBFB_EBUSY;
-        if (wait_ms < 0) s->done_cv.wait(l, finished);
-        else if (!s->done_cv.wait_for(l, std::chrono::milliseconds(wait_ms), finished))
-            return RBFB_ETIMEOUT;
+    Req* r = nullptr;
+    {
+        std::unique_lock<std::mutex> l(s->mu);
+        auto it = s->reqs.find(ticket);
+        if (it == s->reqs.end()) return RBFB_ENOTFOUND;
+        r = it->second.get();
+        auto finished = [&] { return r->state == State::Done || r->state == State::Failed; };
+        if (!finished()) {
+            if (wait_ms == 0) return RBFB_EBUSY;
+            if (wait_ms < 0) s->done_cv.wait(l, finished);
+            else if (!s->done_cv.wait_for(l, std::chrono::milliseconds(wait_ms), finished))
+                return RBFB_ETIMEOUT;
+        }
     }
+    // the request's stream has finished: its counters are final (read once,
+    // without the lock)
     if (r->state == State::Done && !r->counted && r->ctr) {
-        // counters once (the request's stream is finished)
         rbfb::DevCounters h{};
         if (cudaMemcpy(&h, r->ctr, sizeof(h), cudaMemcpyDeviceToHost) == cudaSuccess) {
+            std::lock_guard<std::mutex> l(s->mu);
             r->singular = static_cast<long long>(h.singular);
             r->fallback = h.fb_count;
             r->counted = true;
         }
     }
+    std::lock_guard<std::mutex> l(s->mu);
     if (res) {
         std::memset(res, 0, sizeof(*res));
         res->status = r->state == State::Failed ? r->status : RBFB_OK;

@@ -16,6 +16,11 @@ using namespace rbfb;
 
 extern "C" {
 
+const char* rbfb_variant_name(int index) {
+    const auto& vs = variants();
+    return (index >= 0 && index < static_cast<int>(vs.size())) ? vs[index].name : nullptr;
+}
+
 int rbfb_autotune(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const double* x,
                   const double* y, int k, const int* ja, double* const* values_h) {
     if (!ctx) return RBFB_EINVAL;

@@ -96,6 +96,7 @@ _PROTOS = {
     "rbfb_store_to_csr": (_i, [_i, _vp, _vp, _vp, _vp, _vp]),
     "rbfb_solve_dp": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "rbfb_autotune": (_i, [_vp, C.POINTER(Desc), _i, _vp, _vp, _i, _vp, _vp]),
+    "rbfb_variant_name": (C.c_char_p, [_i]),
     "rbfb_server_create": (_i, [C.POINTER(_vp), _i, C.c_size_t, _i]),
     "rbfb_server_submit": (_i, [_vp, C.POINTER(Request), C.POINTER(_ll)]),
     "rbfb_server_poll": (_i, [_vp, _ll, _i, C.POINTER(Result)]),
@@ -284,6 +285,11 @@ class Context:
         st = lib().rbfb_autotune(self.h, C.byref(desc), x.numel(), _ptr(x), _ptr(y), k,
                                  _ptr(ja), tab)
         return self._check(st, "autotune")
+
+
+def variant_name(index: int):
+    v = lib().rbfb_variant_name(index)
+    return None if v is None else v.decode()
 
 
 def store_to_csr(nstencils, ia, wxx, wyy, va, stream=None):

@@ -78,7 +78,7 @@ typedef struct rbfb_desc {
     int precision;     /* RBFB_FP64 or RBFB_FP32_IR                                 */
     int scale;         /* 1: power-of-two radius scaling of each stencil (exact)    */
     int max_sweeps;    /* refinement sweeps before the FP64 fallback (0 = 6)        */
-    double ir_tol;     /* stop when max|dx| <= ir_tol * max|x| (0 = 1e-13)          */
+    double ir_tol;     /* converged when max|dx| <= ir_tol * max|x| (0 = 1e-11)     */
     double period[2];  /* box sides for minimum-image displacements; 0 = open axis  */
     int nc;            /* number of interpolation points (RBFB_OP_INTERP)           */
     const double* xc;  /* interpolation points in the stencil-local frame (device)  */
@@ -193,6 +193,10 @@ int rbfb_solve_dp(double* A, int* ipiv, double* B, int* info, void* stream);
  * reference's block size comes from cuSolverDx, src/rbf_operators.h:280-281). */
 int rbfb_autotune(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const double* x,
                   const double* y, int k, const int* ja, double* const* values_h);
+
+/* Name of compiled kernel shape `index` (as returned by rbfb_autotune), e.g.
+ * "mix_p3q5_n48_g16x2", or NULL past the last one. */
+const char* rbfb_variant_name(int index);
 
 /* ---- serving ---------------------------------------------------------------- */
 /* Continuous-batching assembly server: requests (node sets of any size) are

@@ -54,11 +54,12 @@ def test_fill_matrices_match_oracle(ctx, torch_cuda):
     d = R.make_desc(P)
     x = T.as_tensor(g["x"]).cuda()
     y = T.as_tensor(g["y"]).cuda()
-    # only the first n stencils: x, y stay complete (neighbours index them)
-    lib = R.lib()
-    st = lib.rbfb_fill_matrices(ctx.h, d, n, x.data_ptr(), y.data_ptr(),
-                                T.as_tensor(ia).cuda().data_ptr(),
-                                T.as_tensor(ja).cuda().data_ptr(), M.data_ptr(), ldm, None)
+    # only the first n stencils: x, y stay complete (neighbours index them);
+    # the device arrays are held in names so they live through the launch
+    iad = T.as_tensor(ia).cuda()
+    jad = T.as_tensor(ja).cuda()
+    st = R.lib().rbfb_fill_matrices(ctx.h, d, n, x.data_ptr(), y.data_ptr(), iad.data_ptr(),
+                                    jad.data_ptr(), M.data_ptr(), ldm, None)
     assert st == 0
     T.cuda.synchronize()
     Mh = M.cpu().numpy().reshape(n, ldm, ldm)
