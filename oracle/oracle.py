@@ -61,6 +61,10 @@ def lib():
         L.orc_num_rhs.argtypes = [C.c_int, C.c_int]
         L.orc_npoly.restype = C.c_int
         L.orc_npoly.argtypes = [C.c_int]
+        L.orc_assemble_fixed_ld.restype = C.c_longlong
+        L.orc_assemble_fixed_ld.argtypes = [C.c_int, _dp, _dp, C.c_int, _ip, C.c_int, C.c_int,
+                                            C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p,
+                                            C.c_void_p]
         L.orc_phs.restype = C.c_double
         L.orc_phs.argtypes = [C.c_int, C.c_double]
         L.orc_set_threads.argtypes = [C.c_int]
@@ -137,6 +141,24 @@ def assemble(x, y, ja, k, P, Q=None, ops=OP_LAPLACE | OP_DX | OP_DY, xc=None, yc
                                   None if xc_a is None else xc_a.ctypes.data,
                                   None if yc_a is None else yc_a.ctypes.data, int(bool(scale)),
                                   Lx, Ly, _ptr_table(out), info.ctypes.data)
+    if rc < 0:
+        raise ValueError("oracle rejected the arguments")
+    return np.stack(out), info
+
+
+def assemble_ld(x, y, ja, k, P, Q=None, ops=OP_LAPLACE | OP_DX | OP_DY, scale=True, period=None):
+    """The same assembly in x87 long double (64-bit significand): a more
+    accurate solution to measure FP64 and refined-FP32 errors against on
+    ill-conditioned stencils. Derivative operators only."""
+    x, y, ja = _f64(x), _f64(y), _i32(ja)
+    n = x.size
+    Q = 2 * P - 1 if Q is None else Q
+    nrhs = num_rhs(ops, 0)
+    out = [np.empty(n * k, np.float64) for _ in range(nrhs)]
+    info = np.zeros(n, np.int32)
+    Lx, Ly = (0.0, 0.0) if period is None else (float(period[0]), float(period[1]))
+    rc = lib().orc_assemble_fixed_ld(n, x, y, k, ja, P, Q, ops, int(bool(scale)), Lx, Ly,
+                                     _ptr_table(out), info.ctypes.data)
     if rc < 0:
         raise ValueError("oracle rejected the arguments")
     return np.stack(out), info

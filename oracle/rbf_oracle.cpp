@@ -537,3 +537,123 @@ void orc_stencil_d2(int n, const double* x, const double* y, int k, const int* j
 }
 
 }  // extern "C"
+
+// ---- extended precision (x87 long double, 64-bit significand) -----------------
+// The same system and elimination in long double, from the same FP64 node
+// coordinates. Used only to measure how far FP64 (and the FP32-refined
+// result) are from a more accurate solution on ill-conditioned stencils.
+namespace {
+
+inline long double phs_ld(int Q, long double r2) {
+    const long double r = sqrtl(r2);
+    long double p = r;
+    for (int i = 0; i < (Q - 1) / 2; ++i) p *= r2;
+    return p;
+}
+
+int assemble_one_ld(const Desc& D, int P, int Q, int s, int k, const int* idx, const double* x,
+                    const double* y, double* const* out, long long out_off) {
+    const int np = npoly(P);
+    const int n = k + np;
+    int col_op[kMaxRhs + 64];
+    const int nrhs = rhs_columns(D.ops, D.nc, col_op);
+    const int W = n + nrhs;
+    std::vector<long double> xs(k), ys(k);
+    double xd[kMaxSys], yd[kMaxSys];
+    for (int j = 0; j < k; ++j) {
+        xd[j] = minimum_image(x[idx[j]] - x[s], D.Lx);
+        yd[j] = minimum_image(y[idx[j]] - y[s], D.Ly);
+    }
+    const int e = D.scale ? scale_exponent(xd, yd, k) : 0;
+    for (int j = 0; j < k; ++j) {
+        xs[j] = ldexpl((long double)xd[j], -e);
+        ys[j] = ldexpl((long double)yd[j], -e);
+    }
+    std::vector<long double> a(static_cast<size_t>(n) * W, 0.0L);
+    auto mono = [&](long double xx, long double yy, long double* b) {
+        long double X[8], Y[8];
+        X[0] = Y[0] = 1.0L;
+        for (int i = 1; i <= P; ++i) { X[i] = X[i - 1] * xx; Y[i] = Y[i - 1] * yy; }
+        int m = 0;
+        for (int d = 0; d <= P; ++d)
+            for (int j = 0; j <= d; ++j) b[m++] = X[d - j] * Y[j];
+    };
+    for (int i = 0; i < k; ++i) {
+        long double* row = &a[static_cast<size_t>(np + i) * W];
+        for (int j = 0; j < k; ++j) {
+            const long double dx = xs[j] - xs[i], dy = ys[j] - ys[i];
+            row[np + j] = phs_ld(Q, dx * dx + dy * dy);
+        }
+        long double b[64];
+        mono(xs[i], ys[i], b);
+        for (int m = 0; m < np; ++m) { row[m] = b[m]; a[m * W + np + i] = b[m]; }
+    }
+    for (int q = 0; q < nrhs; ++q) {
+        const int op = col_op[q];
+        for (int i = 0; i < k; ++i) {
+            const long double xk = xs[i], yk = ys[i];
+            const long double r2 = xk * xk + yk * yk;
+            const long double rq2 = (Q - 2 == 1) ? sqrtl(r2) : phs_ld(Q - 2, r2);
+            const long double qq = Q;
+            long double v = 0.0L;
+            switch (op) {
+                case OP_LAPLACE: v = qq * qq * rq2; break;
+                case OP_DX: v = -qq * rq2 * xk; break;
+                case OP_DY: v = -qq * rq2 * yk; break;
+                default: v = 0.0L; break;
+            }
+            a[(np + i) * W + n + q] = v;
+        }
+        for (int m = 0; m < np; ++m) a[m * W + n + q] = poly_op_at_origin(op, m);
+    }
+    std::vector<char> used(n, 0);
+    std::vector<int> prow(n);
+    for (int c = 0; c < n; ++c) {
+        int p = -1;
+        long double best = -1.0L;
+        for (int r = 0; r < n; ++r)
+            if (!used[r] && fabsl(a[r * W + c]) > best) { best = fabsl(a[r * W + c]); p = r; }
+        if (!(best > 0.0L)) return c + 1;
+        used[p] = 1;
+        prow[c] = p;
+        for (int r = 0; r < n; ++r) {
+            if (used[r]) continue;
+            const long double l = a[r * W + c] / a[p * W + c];
+            a[r * W + c] = l;
+            for (int j = c + 1; j < W; ++j) a[r * W + j] -= l * a[p * W + j];
+        }
+    }
+    std::vector<long double> xsol(static_cast<size_t>(n) * nrhs);
+    for (int c = n - 1; c >= 0; --c) {
+        const int p = prow[c];
+        for (int q = 0; q < nrhs; ++q) xsol[c * nrhs + q] = a[p * W + n + q] / a[p * W + c];
+        for (int t = 0; t < c; ++t) {
+            const int r = prow[t];
+            for (int q = 0; q < nrhs; ++q) a[r * W + n + q] -= a[r * W + c] * xsol[c * nrhs + q];
+        }
+    }
+    for (int q = 0; q < nrhs; ++q) {
+        const int m = op_order(col_op[q]);
+        for (int j = 0; j < k; ++j)
+            out[q][out_off + j] = (double)ldexpl(xsol[(np + j) * nrhs + q], -m * e);
+    }
+    return 0;
+}
+
+}  // namespace
+
+extern "C" long long orc_assemble_fixed_ld(int nstencils, const double* x, const double* y, int k,
+                                           const int* ja, int P, int Q, int ops, int scale,
+                                           double Lx, double Ly, double* const* out, int* info) {
+    Desc D{ops, 0, nullptr, nullptr, scale, Lx, Ly};
+    if ((ops & OP_INTERP) || check_desc(D, P, Q, k) < 0 || nstencils < 0) return -1;
+    long long bad = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : bad)
+    for (int s = 0; s < nstencils; ++s) {
+        const int st = assemble_one_ld(D, P, Q, s, k, ja + static_cast<size_t>(s) * k, x, y, out,
+                                       static_cast<long long>(s) * k);
+        if (info) info[s] = st;
+        bad += (st != 0);
+    }
+    return bad;
+}

@@ -163,3 +163,12 @@ def test_collinear_stencil_is_singular():
     ja = O.knn_brute(x, y, 10)
     W, info = O.assemble(x, y, ja, 10, 2)
     assert (info != 0).all()
+
+
+def test_long_double_agrees_on_well_conditioned_stencils():
+    # the x87 long double solve (64-bit significand) and the FP64 oracle agree
+    # to ~cond * 2^-53 on the degree-2 workload (cond ~ 4e3 scaled)
+    g = golden("square69_k21")
+    W, _ = O.assemble(g["x"], g["y"], g["ja_nanoflann"], 21, 2)
+    Wl, _ = O.assemble_ld(g["x"], g["y"], g["ja_nanoflann"], 21, 2)
+    assert O.max_rel_err(W, Wl, 21).max() < 1e-12
