@@ -30,6 +30,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <mutex>
 
 #include "asm_math.cuh"
 #include "runtime.h"
@@ -608,3 +609,136 @@ int rbfb_knn_status(rbfb_ctx* ctx, void* stream) {
 }
 
 }  // extern "C"
+
+// ---- no-allocation variant: rbfb_knn_stencils_static ------------------------------
+//
+// Some callers may not allocate device memory once they are running: a solver
+// loop that claimed all its device memory in a set-up phase and must not call
+// cudaMalloc/cudaFree afterwards (those calls can synchronise the device and
+// fragment the caller's pool), or a host application whose device memory is
+// owned by another framework's allocator. For them this search keeps its
+// scratch in a fixed array in device memory, defined below, instead of in a
+// context: every GPU that loads the library holds the array until the process
+// exits, and no call allocates anything.
+namespace rbfb {
+namespace knn {
+
+constexpr int kStaticMaxNodes = 65536;                   // largest node set served
+constexpr int kStaticMaxCells = kStaticMaxNodes / kPerCell;  // largest cell grid served
+constexpr size_t al256(size_t b) { return (b + 255) & ~size_t(255); }
+constexpr size_t kS_cell_of = 0;
+constexpr size_t kS_count = kS_cell_of + al256(4ull * kStaticMaxNodes);
+constexpr size_t kS_start = kS_count + al256(4ull * (kStaticMaxCells + 1));
+constexpr size_t kS_cursor = kS_start + al256(4ull * (kStaticMaxCells + 1));
+constexpr size_t kS_bsums = kS_cursor + al256(4ull * (kStaticMaxCells + 1));
+constexpr size_t kS_sidx = kS_bsums + al256(4ull * ((kStaticMaxCells + 1) / kScanBlock + 2));
+constexpr size_t kS_sx = kS_sidx + al256(4ull * kStaticMaxNodes);
+constexpr size_t kS_sy = kS_sx + al256(8ull * kStaticMaxNodes);
+constexpr size_t kS_fx = kS_sy + al256(8ull * kStaticMaxNodes);
+constexpr size_t kS_fy = kS_fx + al256(8ull * kStaticMaxNodes);
+constexpr size_t kS_grid = kS_fy + al256(8ull * kStaticMaxNodes);
+constexpr size_t kS_bbox = kS_grid + al256(sizeof(Grid));
+constexpr size_t kS_status = kS_bbox + al256(4 * sizeof(unsigned long long));
+constexpr size_t kS_total = kS_status + al256(2 * sizeof(int));
+
+// The scratch. In host code this name is only a stand-in for the device
+// array, never a device address: host code takes the address with
+// cudaGetSymbolAddress (per device) and passes it to the kernels.
+static __device__ __align__(256) unsigned char g_knn_static[kS_total];
+
+namespace {
+std::mutex g_static_mu;
+void* g_static_addr[64] = {};  // device address of the array, per device ordinal
+}  // namespace
+
+}  // namespace knn
+}  // namespace rbfb
+
+extern "C" int rbfb_knn_stencils_static(int n, const double* x, const double* y, int k,
+                                        const double* period_h, int* ja, void* stream) {
+    using namespace rbfb::knn;
+    if (!x || !y || !ja) return RBFB_EINVAL;
+    if (n < 1 || k < 1 || k > n || k > kMaxK) return RBFB_EINVAL;
+    const bool periodic = period_h && period_h[0] > 0 && period_h[1] > 0;
+    if (period_h && ((period_h[0] > 0) != (period_h[1] > 0))) return RBFB_EINVAL;
+    if (n > kStaticMaxNodes) return RBFB_ETOOBIG;
+    // the cell grid of the search, as build() forms it
+    int cx, cy;
+    if (periodic) {
+        const double aspect = period_h[0] / period_h[1];
+        const double cells = std::max(1.0, static_cast<double>(n) / kPerCell);
+        cx = std::max(1, static_cast<int>(std::sqrt(cells * aspect)));
+        cy = std::max(1, static_cast<int>(std::sqrt(cells / aspect)));
+    } else {
+        cx = cy = std::max(1, static_cast<int>(std::sqrt(static_cast<double>(n) / kPerCell)));
+    }
+    const long long cells = static_cast<long long>(cx) * cy;
+    if (cells > kStaticMaxCells) return RBFB_ETOOBIG;
+    // set-up, once per device, with that device current
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return RBFB_ECUDA;
+    unsigned char* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_static_mu);
+        if (!g_static_addr[dev]) {
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_knn_static) != cudaSuccess || !p) return RBFB_ECUDA;
+            g_static_addr[dev] = p;
+        }
+        base = static_cast<unsigned char*>(g_static_addr[dev]);
+    }
+    int* cell_of = reinterpret_cast<int*>(base + kS_cell_of);
+    int* count = reinterpret_cast<int*>(base + kS_count);
+    int* start = reinterpret_cast<int*>(base + kS_start);
+    int* cursor = reinterpret_cast<int*>(base + kS_cursor);
+    int* bsums = reinterpret_cast<int*>(base + kS_bsums);
+    int* sidx = reinterpret_cast<int*>(base + kS_sidx);
+    double* sx = reinterpret_cast<double*>(base + kS_sx);
+    double* sy = reinterpret_cast<double*>(base + kS_sy);
+    double* fx = reinterpret_cast<double*>(base + kS_fx);
+    double* fy = reinterpret_cast<double*>(base + kS_fy);
+    Grid* grid = reinterpret_cast<Grid*>(base + kS_grid);
+    unsigned long long* bbox = reinterpret_cast<unsigned long long*>(base + kS_bbox);
+    int* status = reinterpret_cast<int*>(base + kS_status);
+    int* total = status + 1;
+
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int tpb = 256;
+    const int blocks = std::max(1, std::min((n + tpb - 1) / tpb, std::max(sms, 1) * 8));
+    if (periodic) {
+        Grid g{0.0, 0.0, period_h[0] / cx, period_h[1] / cy, cx, cy, period_h[0], period_h[1]};
+        set_grid_kernel<<<1, 1, 0, st>>>(g, grid);
+    } else {
+        bbox_init_kernel<<<1, 1, 0, st>>>(bbox);
+        bbox_kernel<<<blocks, tpb, 0, st>>>(x, y, n, reinterpret_cast<double*>(bbox));
+        grid_kernel<<<1, 1, 0, st>>>(bbox, cx, cy, grid);
+    }
+    // what must start at zero: the per-cell counters and the status word
+    if (cudaMemsetAsync(count, 0, (cells + 1) * sizeof(int), st) != cudaSuccess ||
+        cudaMemsetAsync(cursor, 0, (cells + 1) * sizeof(int), st) != cudaSuccess ||
+        cudaMemsetAsync(status, 0, sizeof(int), st) != cudaSuccess)
+        return RBFB_ECUDA;
+    cell_count_kernel<<<blocks, tpb, 0, st>>>(x, y, n, grid, cell_of, count, fx, fy);
+    const int ncell1 = static_cast<int>(cells) + 1;
+    const int nsb = (ncell1 + kScanBlock - 1) / kScanBlock;
+    scan_block_kernel<<<nsb, kScanBlock, 0, st>>>(count, start, ncell1, bsums);
+    scan_sums_kernel<<<1, 1, 0, st>>>(bsums, nsb, total);
+    scan_add_kernel<<<nsb, kScanBlock, 0, st>>>(start, ncell1, bsums);
+    scatter_kernel<<<blocks, tpb, 0, st>>>(cell_of, n, start, cursor, fx, fy, sidx, sx, sy);
+    QueryArgs a{};
+    a.g = grid;
+    a.start = start;
+    a.sidx = sidx;
+    a.sx = sx;
+    a.sy = sy;
+    a.nq = n;
+    a.qorder = sidx;
+    a.k = k;
+    a.ja = ja;
+    a.status = status;
+    const int qblocks = std::max(1, std::min((n + kWarps - 1) / kWarps, std::max(sms, 1) * 16));
+    query_kernel<<<qblocks, kWarps * 32, 0, st>>>(a);
+    return cudaGetLastError() == cudaSuccess ? RBFB_OK : RBFB_ECUDA;
+}

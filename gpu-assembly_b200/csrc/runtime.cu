@@ -266,6 +266,7 @@ const char* rbfb_status_string(int status) {
         case RBFB_EBUDGET: return "request exceeds the memory budget";
         case RBFB_ENOTFOUND: return "unknown ticket";
         case RBFB_EBUSY: return "not finished";
+        case RBFB_ETOOBIG: return "problem exceeds the fixed scratch of the no-allocation call";
         default: return status > 0 ? "singular stencils" : "unknown status";
     }
 }

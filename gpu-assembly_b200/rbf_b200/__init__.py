@@ -27,8 +27,9 @@ import numpy as np
 PKG = Path(__file__).resolve().parent.parent
 LIB_PATH = PKG / "lib" / "librbf_b200.so"
 
-OK, EINVAL, ECUDA, ENOMEM, EUNSUPPORTED, ETIMEOUT, EBUDGET, ENOTFOUND, EBUSY = (
-    0, -1, -2, -3, -4, -5, -6, -7, -8)
+OK, EINVAL, ECUDA, ENOMEM, EUNSUPPORTED, ETIMEOUT, EBUDGET, ENOTFOUND, EBUSY, ETOOBIG = (
+    0, -1, -2, -3, -4, -5, -6, -7, -8, -9)
+STATIC_MAX_NODES = 65536  # limit of rbfb_knn_stencils_static
 OP_INTERP, OP_LAPLACE, OP_DX, OP_DY, OP_DXX, OP_DYY, OP_DXY = 1, 2, 4, 8, 16, 32, 64
 FP64, FP32_IR = 0, 1
 MAX_RHS = 8
@@ -86,6 +87,7 @@ _PROTOS = {
     "rbfb_knn_stencils": (_i, [_vp, _i, _vp, _vp, _i, _vp, _vp, _vp]),
     "rbfb_knn_query": (_i, [_vp, _i, _vp, _vp, _i, _vp, _vp, _i, _vp, _vp, _vp]),
     "rbfb_knn_status": (_i, [_vp, _vp]),
+    "rbfb_knn_stencils_static": (_i, [_i, _vp, _vp, _i, _vp, _vp, _vp]),
     "rbfb_assemble": (_i, [_vp, C.POINTER(Desc), _i, _vp, _vp, _i, _vp, _vp, _vp,
                            C.POINTER(Stats), _vp]),
     "rbfb_assemble_csr": (_i, [_vp, C.POINTER(Desc), _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
@@ -285,6 +287,16 @@ class Context:
         st = lib().rbfb_autotune(self.h, C.byref(desc), x.numel(), _ptr(x), _ptr(y), k,
                                  _ptr(ja), tab)
         return self._check(st, "autotune")
+
+
+def knn_stencils_static(x, y, k, ja, period=None, stream=None):
+    """rbfb_knn_stencils_static: the k-NN search without any allocation
+    (fixed device scratch, n <= STATIC_MAX_NODES). Raises RbfError."""
+    n = x.numel()
+    per = None if period is None else (C.c_double * 2)(*period)
+    st = lib().rbfb_knn_stencils_static(n, _ptr(x), _ptr(y), k, per, _ptr(ja), _stream(stream))
+    if st != OK:
+        raise RbfError(st, status_string(st))
 
 
 def variant_name(index: int):

@@ -45,6 +45,7 @@ extern "C" {
 #define RBFB_EBUDGET (-6)     /* request larger than the server's HBM budget   */
 #define RBFB_ENOTFOUND (-7)   /* unknown ticket                                */
 #define RBFB_EBUSY (-8)       /* ticket not finished (non-blocking poll)       */
+#define RBFB_ETOOBIG (-9)     /* beyond the fixed scratch of a no-allocation call */
 
 /* ---- operators (right-hand sides) --------------------------------------
  * Right-hand-side columns, in output order: nc interpolation points first
@@ -124,6 +125,25 @@ int rbfb_knn_stencils(rbfb_ctx* ctx, int n, const double* x, const double* y, in
 int rbfb_knn_query(rbfb_ctx* ctx, int n, const double* x, const double* y, int nq,
                    const double* xq, const double* yq, int k, const double* period_h, int* ja,
                    void* stream);
+
+/* The search of rbfb_knn_stencils without any allocation, for callers that
+ * may not allocate device memory while they run: a solver loop that claimed
+ * its device memory in a set-up phase and must not call cudaMalloc/cudaFree
+ * afterwards (they can synchronise the device and fragment its pool), or a
+ * host whose device memory belongs to another framework's allocator. No
+ * counterpart in the reference (its searches run on the host).
+ *
+ * Needs no context: the scratch is a fixed array of about 3 MB in device
+ * memory, held by every GPU that loads this library until the process exits.
+ * Limit: n <= 65,536 nodes (and a cell grid of at most n/2 cells); larger
+ * problems are rejected with RBFB_ETOOBIG. The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress) with that device
+ * current; make that first call before any stream capture. All calls share
+ * the one array: calls whose work overlaps on the GPU (other streams, other
+ * host threads) race and must be serialised by the caller. Same arguments,
+ * result and ordering as rbfb_knn_stencils. */
+int rbfb_knn_stencils_static(int n, const double* x, const double* y, int k,
+                             const double* period_h, int* ja, void* stream);
 
 /* Completion status of the last search on this context: 0 when every query
  * finished, 1 when a query gave up widening its search (its row of ja is

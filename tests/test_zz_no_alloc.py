@@ -1,0 +1,52 @@
+"""rbfb_knn_stencils_static, the k-NN search that allocates nothing.
+
+It is meant for callers that may not allocate device memory while running
+(a solver loop past its set-up phase, a host whose device memory belongs to
+another allocator). Checked here through the C ABI against the ordinary
+entry point rbfb_knn_stencils: the stencils are integer indices, so the two
+must agree exactly, and they must keep agreeing on a second call in a row
+(the fixed scratch keeps the previous call's contents). This file is named
+to be collected last.
+"""
+import numpy as np
+import pytest
+
+import rbf_b200 as R
+from rbf_b200 import nodesets as NS
+
+pytestmark = pytest.mark.gpu
+
+
+def _cases():
+    x, y, _ = NS.jittered_grid(69, 0.3, seed=1)                 # open plane, 4,761 nodes
+    yield x, y, 21, None
+    x, y, _ = NS.jittered_grid(200, 0.3, seed=8, periodic=True)  # periodic, 40,000 nodes
+    yield x, y, 35, (1.0, 1.0)
+    x, y, _ = NS.gaussian_bump(20000, seed=4)                   # non-uniform density
+    yield x, y, 64, None
+
+
+def test_static_search_matches_the_ordinary_one(torch_cuda):
+    T = torch_cuda
+    with R.Context(0) as ctx:
+        for x, y, k, period in _cases():
+            n = x.size
+            xd, yd = T.as_tensor(x).cuda(), T.as_tensor(y).cuda()
+            ref = T.full((n * k,), -1, dtype=T.int32, device="cuda")
+            ctx.knn_stencils(xd, yd, k, ref, period=period)
+            for call in range(2):  # two calls in a row on the same scratch
+                ja = T.full((n * k,), -1, dtype=T.int32, device="cuda")
+                R.knn_stencils_static(xd, yd, k, ja, period=period)
+                T.cuda.synchronize()
+                np.testing.assert_array_equal(ja.cpu().numpy(), ref.cpu().numpy(),
+                                              err_msg=f"call {call}, n={n}, k={k}")
+
+
+def test_static_search_rejects_oversize(torch_cuda):
+    T = torch_cuda
+    n = R.STATIC_MAX_NODES + 1
+    x = T.rand(n, dtype=T.float64, device="cuda")
+    ja = T.empty(n * 4, dtype=T.int32, device="cuda")
+    with pytest.raises(R.RbfError) as e:
+        R.knn_stencils_static(x, x, 4, ja)
+    assert e.value.status == R.ETOOBIG
