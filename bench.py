@@ -184,10 +184,10 @@ def reference_arm(args):
     return 0
 
 
-def traffic_per_launch():
+def traffic_per_launch(form):
     """DRAM bytes per launch of the dominant kernel, from the committed ncu
     summary (profiles/), scaled to the full workload; None if absent."""
-    p = ROOT / "profiles" / "asm_mixed_periodic1024.txt"
+    p = ROOT / "profiles" / f"asm_{form}_periodic1024.txt"
     if not p.exists():
         return None
     for ln in p.read_text().splitlines():
@@ -308,8 +308,8 @@ def main():
 
     # ---- timed: mixed (headline) and FP64 on the same node set
     with Clocks(local) as clk:
-        ms_mix, launches = timed(d_mix, args.steps, args.warmup)
-    ms_64, _ = timed(d_f64, max(3, args.steps // 2), args.warmup)
+        ms_64, launches = timed(d_f64, args.steps, args.warmup)
+        ms_mix, _ = timed(d_mix, args.steps, args.warmup)
     # dominant kernel alone: the assembly (k-NN excluded), CUDA events on its stream
     step(d_mix)
     torch.cuda.synchronize()
@@ -340,13 +340,14 @@ def main():
     vh = [torch.empty(nk, dtype=torch.float64).pin_memory() for _ in range(NRHS)]
     jh = torch.empty(nk, dtype=torch.int32).pin_memory()
     e2e_steps = max(3, args.steps // 2)
+    d_head = d_f64 if ms_64 <= ms_mix else d_mix  # the faster form (both meet the bound here)
     for _ in range(2):
-        ctx.assemble_host(d_mix, xh, yh, K, vh, ja_out_h=jh)
+        ctx.assemble_host(d_head, xh, yh, K, vh, ja_out_h=jh)
     barrier()
     t0 = time.perf_counter()
     e2e_dev_ms = 0.0
     for _ in range(e2e_steps):
-        st = ctx.assemble_host(d_mix, xh, yh, K, vh, ja_out_h=jh)
+        st = ctx.assemble_host(d_head, xh, yh, K, vh, ja_out_h=jh)
         e2e_dev_ms += st["ms"]
     t1 = time.perf_counter()
     barrier()
@@ -363,47 +364,59 @@ def main():
         return 0
     pk, src = peaks()
     flops = FLOP_PER_STENCIL * n
-    achieved = flops / (ms_asm * 1e-3) / 1e12
-    fp32_peak, fp32_src = fp32_peak_tflops()
+    # headline: the faster of the two forms that meet the 1e-10 bound
+    ok = {"mixed": err_mix <= 1e-10, "fp64": err_64 <= 1e-10}
+    rate = {"mixed": n / (ms_mix * 1e-3), "fp64": n / (ms_64 * 1e-3)}
+    form = max((f for f in ("mixed", "fp64") if ok[f]), key=lambda f: rate[f], default="fp64")
+    ms_head = ms_mix if form == "mixed" else ms_64
+    ms_kernel = ms_asm if form == "mixed" else ms_asm64
+    pipe = "fp32" if form == "mixed" else "fp64"
+    peak_pipe, peak_src = pipe_peak_tflops(pipe)
+    achieved = flops / (ms_kernel * 1e-3) / 1e12
     line = {
         "metric": "stencils/s k=35 deg3 (periodic 1024^2 jittered grid, 3 operators)",
-        "value": ws * n / (ms_mix * 1e-3),
+        "value": ws * n / (ms_head * 1e-3),
         "unit": "stencils/s",
         "n_gpus": ws,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": ms_mix,
+        "ms_per_step": ms_head,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32+f64",
+        "dtype": "f64" if form == "fp64" else "f32+f64",
         "data": "synthetic (seeded jittered grid, numpy default_rng)",
         "config": {"workload": f"periodic {m}x{m} jittered grid (+-0.3h), k={K} k-NN + "
-                               f"assembly, PHS r^{Q} + degree {P} (n={N_SYS}), Laplacian/dx/dy, "
-                               "FP32 LU + FP64 refinement",
+                               f"assembly, PHS r^{Q} + degree {P} (n={N_SYS}), Laplacian/dx/dy",
                    "stencils_per_gpu": n, "l2": "inputs and outputs > L2 every step",
-                   "precision": "FP32 factorisation + FP64 residual refinement, FP64 fallback"},
-        "fp64": {"stencils_per_s": ws * n / (ms_64 * 1e-3), "ms_per_step": ms_64,
-                 "asm_ms": ms_asm64},
+                   "form": form,
+                   "forms": {"fp64": "FP64 fill + FP64 elimination (bit-identical to the oracle)",
+                             "mixed": "FP32 elimination + FP64 residual refinement, FP64 "
+                                      "fallback per stencil"}},
+        "mixed": {"stencils_per_s": ws * rate["mixed"], "ms_per_step": ms_mix,
+                  "asm_ms": ms_asm, "max_rel_weight_err": err_mix,
+                  "fallback_stencils": st_mix["fallback"] if st_mix else None,
+                  "sweeps_mean": (st_mix["sweeps"] / max(1, n)) if st_mix else None},
+        "fp64": {"stencils_per_s": ws * rate["fp64"], "ms_per_step": ms_64, "asm_ms": ms_asm64,
+                 "max_rel_weight_err": err_64},
         "mixed_over_fp64": ms_64 / ms_mix,
-        "max_rel_weight_err": {"mixed": err_mix, "fp64": err_64,
-                               "vs": "FP64 CPU oracle, 2048 sampled stencils"},
-        "fallback_stencils": st_mix["fallback"] if st_mix else None,
-        "sweeps_mean": (st_mix["sweeps"] / max(1, n)) if st_mix else None,
+        "max_rel_weight_err_vs": "FP64 CPU oracle, 2048 sampled stencils",
         "stages_ms": {"knn": ms_knn, "assembly_mixed": ms_asm, "assembly_fp64": ms_asm64},
         "e2e": {"value": ws * n / (e2e_ms * 1e-3), "unit": "stencils/s",
                 "h2d_bytes_per_step": 16 * n,
                 "d2h_bytes_per_step": nk * (8 * NRHS + 4),
-                "device_ms": e2e_dev_ms / e2e_steps},
+                "device_ms": e2e_dev_ms / e2e_steps,
+                "form": "fp64" if d_head is d_f64 else "mixed"},
         "gpu_launches": launches,
         "kernel_shapes": tuned,
-        "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
-                     "unit": "TFLOP/s", "frac": achieved / fp32_peak,
-                     "traffic": traffic_per_launch(),
-                     "peak_source": fp32_src,
+        "roofline": {"bound": pipe, "achieved": achieved, "peak": peak_pipe,
+                     "unit": "TFLOP/s", "frac": achieved / peak_pipe,
+                     "traffic": traffic_per_launch(form),
+                     "peak_source": peak_src,
+                     "kernel": f"assembly ({form}), k-NN excluded",
                      "flop_per_stencil": FLOP_PER_STENCIL,
                      "hbm": {"algorithmic_bytes": n * (44 * K + 16),
-                             "achieved_gbs": n * (44 * K + 16) / (ms_asm * 1e-3) / 1e9,
+                             "achieved_gbs": n * (44 * K + 16) / (ms_kernel * 1e-3) / 1e9,
                              "peak_gbs": pk.get("hbm_gbs"), "peak_source": src}},
         "clocks": clk.summary(),
     }
@@ -418,15 +431,16 @@ def main():
     return 0
 
 
-def fp32_peak_tflops():
-    """FP32 FMA peak of this GPU: 2 flops x 128 lanes x SMs x max SM clock
-    (the CUDA-core rate the assembly kernel is bound by)."""
+def pipe_peak_tflops(pipe):
+    """CUDA-core peak of this GPU for the pipe the assembly is bound by: 2
+    flops x (128 FP32 | 64 FP64) FMA lanes x SMs x max SM clock."""
     import torch
     props = torch.cuda.get_device_properties(torch.cuda.current_device())
     pk, _ = peaks()
     mhz = pk.get("sm_max_mhz") or 1965.0
-    return 2 * 128 * props.multi_processor_count * mhz * 1e6 / 1e12, \
-        f"nominal: 2 x 128 FP32 lanes x {props.multi_processor_count} SMs x {mhz:.0f} MHz"
+    lanes = 128 if pipe == "fp32" else 64
+    return 2 * lanes * props.multi_processor_count * mhz * 1e6 / 1e12, \
+        f"nominal: 2 x {lanes} {pipe.upper()} FMA lanes x {props.multi_processor_count} SMs x {mhz:.0f} MHz"
 
 
 def serve_sample(R, NS, device, count):

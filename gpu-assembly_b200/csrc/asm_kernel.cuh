@@ -66,6 +66,7 @@ struct AsmParams {
     const int* ja;  // fixed width: row s at ja + s*k; CSR: ja + ia[s]
     const int* ia;  // nullptr for fixed width
     int k;          // fixed width stencil size
+    int row_base;   // fixed width: ja, values and info hold rows row_base.. only
     double Lx, Ly;  // periods (<= 0: open axis)
     int scale;
     int nrhs;
@@ -336,7 +337,7 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, char* sm
     double* b64 = reinterpret_cast<double*>(smem + C::off_b64);
 
     const int lr = lg / GC, lc = lg % GC;
-    const int off = p.ia ? p.ia[s] : s * p.k;
+    const int off = p.ia ? p.ia[s] : (s - p.row_base) * p.k;
     const int ks = p.ia ? p.ia[s + 1] - off : p.k;
     const int n = NP + ks;
 
@@ -699,7 +700,7 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, char* sm
                 dst[j] = bad ? __longlong_as_double(0x7ff8000000000000ll) : scalbn(v, sh);
             }
         }
-        if (lg == 0 && p.info) p.info[s] = info;
+        if (lg == 0 && p.info) p.info[s - p.row_base] = info;
     } else {
         // ---- FP64 iterative refinement
         for (int i = lg; i < NTP * NRHS; i += G) x64[i] = static_cast<double>(X[i]);
@@ -836,7 +837,7 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, char* sm
                 const int sh = -op_order(p.col_op[q]) * e;
                 for (int j = lg; j < ks; j += G) dst[j] = scalbn(x64[(NP + j) * NRHS + q], sh);
             }
-            if (lg == 0 && p.info) p.info[s] = 0;
+            if (lg == 0 && p.info) p.info[s - p.row_base] = 0;
         }
     }
     __syncwarp(gmask);

@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cstring>
 #include <vector>
 
@@ -28,7 +29,9 @@ constexpr int kTabN = 161;  // system sizes 0..160
 
 struct BatchState {
     int* table = nullptr;     // [5][kTabN] variant per (P, n), -1 = none
-    int table_mixed = -1, table_phs = -1;
+    int table_mixed = -1, table_phs = -1, table_pmin = -1, table_pmax = -1;
+    size_t table_tuned = 0;   // size of the context's tuned table when built
+    std::vector<int> table_used;
     int* counts = nullptr;    // [kMaxVariants] x 3: counts | offsets | cursors
     DevCounters* ctrs = nullptr;  // per bucket
     int* err = nullptr;
@@ -38,7 +41,7 @@ struct BatchState {
     // cached graph of the last batch
     cudaGraphExec_t graph = nullptr;
     std::vector<unsigned char> graph_key;
-    cudaStream_t cap_stream = nullptr;
+    long long graph_launches = 0;  // kernels in the graph
 };
 
 BatchState* state(rbfb_ctx* ctx) {
@@ -102,6 +105,11 @@ int ensure(rbfb_ctx* ctx, BatchState* b, size_t n) {
 // the set of variants that can occur for the allowed degrees.
 int build_table(rbfb_ctx* ctx, BatchState* b, bool mixed, int phs, int Pmin, int Pmax,
                 std::vector<int>& used) {
+    if (b->table_mixed == (mixed ? 1 : 0) && b->table_phs == phs && b->table_pmin == Pmin &&
+        b->table_pmax == Pmax && b->table_tuned == ctx->tuned.size()) {
+        used = b->table_used;  // unchanged: no upload
+        return RBFB_OK;
+    }
     std::vector<int> tab(5 * kTabN, -1);
     used.clear();
     for (int P = 0; P <= 4; ++P)
@@ -115,8 +123,12 @@ int build_table(rbfb_ctx* ctx, BatchState* b, bool mixed, int phs, int Pmin, int
                 used.push_back(v);
         }
     RBFB_CUDA(ctx, cudaMemcpy(b->table, tab.data(), tab.size() * sizeof(int), cudaMemcpyHostToDevice));
-    b->table_mixed = mixed;
+    b->table_mixed = mixed ? 1 : 0;
     b->table_phs = phs;
+    b->table_pmin = Pmin;
+    b->table_pmax = Pmax;
+    b->table_tuned = ctx->tuned.size();
+    b->table_used = used;
     return RBFB_OK;
 }
 
@@ -124,7 +136,6 @@ void release(BatchState* b) {
     cudaFree(b->table); cudaFree(b->counts); cudaFree(b->ctrs); cudaFree(b->err);
     cudaFree(b->bucket_of); cudaFree(b->list);
     if (b->graph) cudaGraphExecDestroy(b->graph);
-    if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
     delete b;
 }
 
@@ -190,19 +201,31 @@ int rbfb_assemble_csr(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const
     }
     const int nb = static_cast<int>(variants().size());
     if (nb > kMaxVariants) return fail(ctx, RBFB_EUNSUPPORTED, "too many compiled shapes");
-    RBFB_CUDA(ctx, cudaMemsetAsync(b->counts, 0, 3 * kMaxVariants * sizeof(int), st));
-    RBFB_CUDA(ctx, cudaMemsetAsync(b->ctrs, 0, kMaxVariants * sizeof(DevCounters), st));
-    RBFB_CUDA(ctx, cudaMemsetAsync(b->err, 0, sizeof(int), st));
-    if (nstencils > 0) {
+    // occupancy queries and shared-memory opt-ins before any capture
+    for (int v : used) {
+        if (grid_for(ctx, v) < 0) return RBFB_ECUDA;
+        if (mixed) {
+            const auto& var = variants()[v];
+            const int v64 = pick_variant(ctx, false, var.P, var.Q, var.ntp);
+            if (v64 < 0) return fail(ctx, RBFB_EUNSUPPORTED, "no FP64 fallback kernel");
+            if (grid_for(ctx, v64) < 0) return RBFB_ECUDA;
+        }
+        if (nrhs > variants()[v].nrhs) return fail(ctx, RBFB_EUNSUPPORTED, "too many right-hand sides");
+    }
+    // the whole batch: a fixed sequence of launches, sizes read on the device
+    auto enqueue = [&](cudaStream_t s) -> int {
+        RBFB_CUDA(ctx, cudaMemsetAsync(b->counts, 0, 3 * kMaxVariants * sizeof(int), s));
+        RBFB_CUDA(ctx, cudaMemsetAsync(b->ctrs, 0, kMaxVariants * sizeof(DevCounters), s));
+        RBFB_CUDA(ctx, cudaMemsetAsync(b->err, 0, sizeof(int), s));
+        if (nstencils == 0) return RBFB_OK;
         const int blocks = std::max(1, std::min((nstencils + 255) / 256, ctx->sms * 8));
-        assign_kernel<<<blocks, 256, 0, st>>>(nstencils, ia, degree, desc->degree, b->table,
-                                              b->bucket_of, b->counts, b->err);
-        offsets_kernel<<<1, 1, 0, st>>>(b->counts, nb);
-        scatter_kernel<<<blocks, 256, 0, st>>>(nstencils, b->bucket_of, b->counts, b->list);
+        assign_kernel<<<blocks, 256, 0, s>>>(nstencils, ia, degree, desc->degree, b->table,
+                                             b->bucket_of, b->counts, b->err);
+        offsets_kernel<<<1, 1, 0, s>>>(b->counts, nb);
+        scatter_kernel<<<blocks, 256, 0, s>>>(nstencils, b->bucket_of, b->counts, b->list);
         ctx->launches += 3;
         RBFB_CUDA(ctx, cudaGetLastError());
         for (int v : used) {
-            if (nrhs > variants()[v].nrhs) return fail(ctx, RBFB_EUNSUPPORTED, "too many right-hand sides");
             AsmParams q = p;
             q.nitems_dev = b->counts + v;
             q.list_off_dev = b->counts + kMaxVariants + v;
@@ -210,20 +233,63 @@ int rbfb_assemble_csr(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const
             q.fb_count = &b->ctrs[v].fb_count;
             q.sweeps_max = &b->ctrs[v].sweeps_max;
             q.sweeps_sum = &b->ctrs[v].sweeps_sum;
-            rc = launch_variant(ctx, v, q, st);
-            if (rc) return rc;
+            int r = launch_variant(ctx, v, q, s);
+            if (r) return r;
             if (mixed) {
                 const auto& var = variants()[v];
-                const int v64 = pick_variant(ctx, false, var.P, var.Q, var.ntp);
-                if (v64 < 0) return fail(ctx, RBFB_EUNSUPPORTED, "no FP64 fallback kernel");
                 AsmParams f = q;
                 f.list = ctx->fb_list;
                 f.nitems_dev = &b->ctrs[v].fb_count;
                 f.fb_list = nullptr;
-                rc = launch_variant(ctx, v64, f, st);
-                if (rc) return rc;
+                r = launch_variant(ctx, pick_variant(ctx, false, var.P, var.Q, var.ntp), f, s);
+                if (r) return r;
             }
         }
+        return RBFB_OK;
+    };
+    // Captured into a CUDA graph on a non-default stream, replayed while the
+    // arguments (and the context's buffers) stay the same.
+    if (st != nullptr) {
+        std::vector<unsigned char> key;
+        auto put = [&](const void* q, size_t len) {
+            const auto* c = static_cast<const unsigned char*>(q);
+            key.insert(key.end(), c, c + len);
+        };
+        const void* ptrs[] = {x, y, ia, ja, degree, info, b->list, b->bucket_of, b->counts,
+                              b->ctrs, ctx->fb_list, b->table};
+        put(ptrs, sizeof(ptrs));
+        put(p.values, sizeof(p.values));
+        put(&nstencils, sizeof(nstencils));
+        put(desc, offsetof(rbfb_desc, nc));
+        put(&desc->nc, sizeof(desc->nc));
+        if (!b->graph || key != b->graph_key) {
+            if (b->graph) cudaGraphExecDestroy(b->graph);
+            b->graph = nullptr;
+            const long long l0 = ctx->launches.load();
+            RBFB_CUDA(ctx, cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            rc = enqueue(st);
+            cudaGraph_t g = nullptr;
+            const cudaError_t ec = cudaStreamEndCapture(st, &g);
+            if (rc) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            if (ec != cudaSuccess) return cuda_fail(ctx, ec, "cudaStreamEndCapture");
+            const cudaError_t ei = cudaGraphInstantiate(&b->graph, g, 0);
+            cudaGraphDestroy(g);
+            if (ei != cudaSuccess) {
+                b->graph = nullptr;
+                return cuda_fail(ctx, ei, "cudaGraphInstantiate");
+            }
+            b->graph_key = key;
+            b->graph_launches = ctx->launches.load() - l0;
+            ctx->launches -= b->graph_launches;  // counted when the graph runs
+        }
+        RBFB_CUDA(ctx, cudaGraphLaunch(b->graph, st));
+        ctx->launches += b->graph_launches;
+    } else {
+        rc = enqueue(st);
+        if (rc) return rc;
     }
     if (!stats) return RBFB_OK;
     std::vector<DevCounters> h(nb);

@@ -216,7 +216,7 @@ struct EventPair {
 
 int enqueue_fixed(rbfb_ctx* ctx, const rbfb_desc* desc, int first, int count, const double* x,
                   const double* y, int k, const int* ja, double* const* values, int* info,
-                  DevCounters* ctr, int* fb, cudaStream_t st) {
+                  DevCounters* ctr, int* fb, cudaStream_t st, int row_base) {
     const int P = desc->degree;
     const int Q = desc->phs ? desc->phs : 2 * P - 1;
     const int n = k + npoly(P);
@@ -233,6 +233,7 @@ int enqueue_fixed(rbfb_ctx* ctx, const rbfb_desc* desc, int first, int count, co
         return fail(ctx, RBFB_EUNSUPPORTED, "more right-hand sides than the compiled kernels hold");
     p.k = k;
     p.item_base = first;
+    p.row_base = row_base;
     if (count == 0) return RBFB_OK;
     if (!mixed) return launch_variant(ctx, v, p, st);
     p.fb_list = fb;
@@ -338,6 +339,35 @@ int rbfb_assemble(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const dou
                        ctx->fb_list, st);
     if (rc) return rc;
     return finish_stats(ctx, info, nstencils, stats, st, ev.a, ev.b, 1);
+}
+
+int rbfb_assemble_range(rbfb_ctx* ctx, const rbfb_desc* desc, int first, int count, int n,
+                        const double* x, const double* y, int k, const int* ja_rows,
+                        double* const* values_rows, int* info_rows, rbfb_stats* stats,
+                        void* stream) {
+    if (!ctx) return RBFB_EINVAL;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    int rc = check_desc(ctx, desc);
+    if (rc) return rc;
+    if (first < 0 || count < 0 || first + count > n || k < 1)
+        return fail(ctx, RBFB_EINVAL, "need 0 <= first, first + count <= n, k >= 1");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    RBFB_CUDA(ctx, cudaSetDevice(ctx->device));
+    EventPair ev;
+    if (stats) {
+        RBFB_CUDA(ctx, cudaEventCreate(&ev.a));
+        RBFB_CUDA(ctx, cudaEventCreate(&ev.b));
+        RBFB_CUDA(ctx, cudaEventRecord(ev.a, st));
+    }
+    RBFB_CUDA(ctx, cudaMemsetAsync(ctx->ctr, 0, sizeof(DevCounters), st));
+    if (desc->precision == RBFB_FP32_IR) {
+        rc = ensure_fb(ctx, static_cast<size_t>(std::max(count, 1)));
+        if (rc) return rc;
+    }
+    rc = enqueue_fixed(ctx, desc, first, count, x, y, k, ja_rows, values_rows, info_rows, ctx->ctr,
+                       ctx->fb_list, st, first);
+    if (rc) return rc;
+    return finish_stats(ctx, info_rows, count, stats, st, ev.a, ev.b, 1);
 }
 
 }  // extern "C"

@@ -90,7 +90,7 @@ int count_singular(rbfb_ctx* ctx, const int* info, int n, unsigned long long* ou
 // counters `ctr` and the fallback region fb (count entries). No sync.
 int enqueue_fixed(rbfb_ctx* ctx, const rbfb_desc* desc, int first, int count, const double* x,
                   const double* y, int k, const int* ja, double* const* values, int* info,
-                  DevCounters* ctr, int* fb, cudaStream_t st);
+                  DevCounters* ctr, int* fb, cudaStream_t st, int row_base = 0);
 
 int check_desc(rbfb_ctx* ctx, const rbfb_desc* d);
 

@@ -90,12 +90,15 @@ _PROTOS = {
     "rbfb_knn_stencils_static": (_i, [_i, _vp, _vp, _i, _vp, _vp, _vp]),
     "rbfb_assemble": (_i, [_vp, C.POINTER(Desc), _i, _vp, _vp, _i, _vp, _vp, _vp,
                            C.POINTER(Stats), _vp]),
+    "rbfb_assemble_range": (_i, [_vp, C.POINTER(Desc), _i, _i, _i, _vp, _vp, _i, _vp, _vp, _vp,
+                                 C.POINTER(Stats), _vp]),
     "rbfb_assemble_csr": (_i, [_vp, C.POINTER(Desc), _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                C.POINTER(Stats), _vp]),
     "rbfb_assemble_host": (_i, [_vp, C.POINTER(Desc), _i, _vp, _vp, _i, _vp, _vp, _vp, _vp,
                                 C.POINTER(Stats)]),
     "rbfb_fill_matrices": (_i, [_vp, C.POINTER(Desc), _i, _vp, _vp, _vp, _vp, _vp, _i, _vp]),
     "rbfb_store_to_csr": (_i, [_i, _vp, _vp, _vp, _vp, _vp]),
+    "rbfb_spmv": (_i, [_i, _i, _vp, _vp, _vp, _vp, _vp, _i, _vp]),
     "rbfb_solve_dp": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "rbfb_autotune": (_i, [_vp, C.POINTER(Desc), _i, _vp, _vp, _i, _vp, _vp]),
     "rbfb_variant_name": (C.c_char_p, [_i]),
@@ -248,6 +251,18 @@ class Context:
         self._check(st, "assemble")
         return s.as_dict() if s is not None else None
 
+    def assemble_range(self, desc: Desc, first, count, x, y, k, ja_rows, values_rows,
+                       info_rows=None, stats=False, stream=None):
+        """Stencils first..first+count-1 of the node set (x, y): ja_rows and
+        values_rows hold only those rows."""
+        tab = (C.c_void_p * len(values_rows))(*[_ptr(v) for v in values_rows])
+        s = Stats() if stats else None
+        st = lib().rbfb_assemble_range(self.h, C.byref(desc), first, count, x.numel(), _ptr(x),
+                                       _ptr(y), k, _ptr(ja_rows), tab, _ptr(info_rows),
+                                       C.byref(s) if s is not None else None, _stream(stream))
+        self._check(st, "assemble_range")
+        return s.as_dict() if s is not None else None
+
     def assemble_csr(self, desc: Desc, x, y, ia, ja, values, degree=None, info=None,
                      stats=False, stream=None):
         n = x.numel()
@@ -302,6 +317,15 @@ def knn_stencils_static(x, y, k, ja, period=None, stream=None):
 def variant_name(index: int):
     v = lib().rbfb_variant_name(index)
     return None if v is None else v.decode()
+
+
+def spmv(n, k, ja, values, u, out, bnd=None, stream=None):
+    """out = A u over the fixed-width CSR (ja, values); out[bnd] = u[bnd]."""
+    nb = 0 if bnd is None else bnd.numel()
+    st = lib().rbfb_spmv(n, k, _ptr(ja), _ptr(values), _ptr(u), _ptr(out), _ptr(bnd), nb,
+                         _stream(stream))
+    if st != OK:
+        raise RbfError(st, "spmv")
 
 
 def store_to_csr(nstencils, ia, wxx, wyy, va, stream=None):

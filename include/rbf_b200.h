@@ -162,6 +162,17 @@ int rbfb_assemble(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const dou
                   const double* y, int k, const int* ja, double* const* values_h, int* info,
                   rbfb_stats* stats, void* stream);
 
+/* Stencils first .. first+count-1 of an n-node set (all n coordinates given):
+ * ja_rows, values_rows[q] and info_rows hold only those rows (row first at
+ * index 0). The unit of the multi-GPU split: each rank assembles a
+ * contiguous node range against the full, replicated node set. The
+ * reference's kernel has no range form (one launch covers all nstencils,
+ * src/rbf_operators.h:317-328). */
+int rbfb_assemble_range(rbfb_ctx* ctx, const rbfb_desc* desc, int first, int count, int n,
+                        const double* x, const double* y, int k, const int* ja_rows,
+                        double* const* values_rows, int* info_rows, rbfb_stats* stats,
+                        void* stream);
+
 /* Ragged stencils in CSR form (ia has nstencils+1 entries), optionally with a
  * per-stencil degree (int8, NULL = desc->degree): the uneven batch. Stencils
  * are bucketed by system size and run in one persistent launch per call,
@@ -204,6 +215,15 @@ int rbfb_store_to_csr(int nstencils, const int* ia, const double* wxx, const dou
  * *info the getrf status. The reference's demo kernel
  * (src/rbf_operators.cpp:7-11, launched from src/main.f90:57). */
 int rbfb_solve_dp(double* A, int* ipiv, double* B, int* info, void* stream);
+
+/* ---- applying the operator -------------------------------------------------- */
+/* out[s] = sum_j values[s*k+j] * u[ja[s*k+j]] for s < n (fused multiply-adds
+ * in row order from zero), then out[bnd[b]] = u[bnd[b]] for the nbnd listed
+ * boundary rows (bnd may be NULL when nbnd = 0). The operator application and
+ * boundary fix the reference sketches after its assembly (A.spmv and the
+ * parallel_for over boundary nodes, src/main.cpp:57-66). */
+int rbfb_spmv(int n, int k, const int* ja, const double* values, const double* u, double* out,
+              const int* bnd, int nbnd, void* stream);
 
 /* ---- tuning --------------------------------------------------------------- */
 /* Times the compiled kernel shapes for one system size and precision on the

@@ -65,6 +65,8 @@ def lib():
         L.orc_assemble_fixed_ld.argtypes = [C.c_int, _dp, _dp, C.c_int, _ip, C.c_int, C.c_int,
                                             C.c_int, C.c_int, C.c_double, C.c_double, C.c_void_p,
                                             C.c_void_p]
+        L.orc_spmv.restype = None
+        L.orc_spmv.argtypes = [C.c_int, C.c_int, _ip, _dp, _dp, _dp, C.c_void_p, C.c_int]
         L.orc_phs.restype = C.c_double
         L.orc_phs.argtypes = [C.c_int, C.c_double]
         L.orc_set_threads.argtypes = [C.c_int]
@@ -263,6 +265,17 @@ def ref_kdtree_stencils(x, y, k, period=None):
     if r.ref_kdtree_stencils(x.size, x, y, k, Lx, Ly, ja) != 0:
         raise ValueError("bad k")
     return ja
+
+
+def spmv(ja, values, u, k, bnd=None):
+    """out = A u (row-order fused multiply-adds from zero), out[bnd] = u[bnd]."""
+    ja, values, u = _i32(ja), _f64(values), _f64(u)
+    n = ja.size // k
+    out = np.empty(n, np.float64)
+    b = None if bnd is None else _i32(bnd)
+    lib().orc_spmv(n, k, ja, values, u, out, None if b is None else b.ctypes.data,
+                   0 if b is None else b.size)
+    return out
 
 
 def max_rel_err(w, w_ref, k):

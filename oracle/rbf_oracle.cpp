@@ -657,3 +657,18 @@ extern "C" long long orc_assemble_fixed_ld(int nstencils, const double* x, const
     }
     return bad;
 }
+
+// Operator application with the boundary fix, in the order the CUDA kernel
+// sums: acc = fma(values[s*k+j], u[ja[s*k+j]], acc) for j = 0..k-1 from zero;
+// then out[bnd[b]] = u[bnd[b]].
+extern "C" void orc_spmv(int n, int k, const int* ja, const double* values, const double* u,
+                         double* out, const int* bnd, int nbnd) {
+#pragma omp parallel for schedule(static)
+    for (int s = 0; s < n; ++s) {
+        double acc = 0.0;
+        for (int j = 0; j < k; ++j)
+            acc = std::fma(values[static_cast<size_t>(s) * k + j], u[ja[static_cast<size_t>(s) * k + j]], acc);
+        out[s] = acc;
+    }
+    for (int b = 0; b < nbnd; ++b) out[bnd[b]] = u[bnd[b]];
+}

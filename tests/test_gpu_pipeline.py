@@ -98,3 +98,80 @@ def test_autotune_picks_a_compiled_shape(ctx, torch_cuda):
     T.cuda.synchronize()
     Wo, _ = O.assemble(g["x"], g["y"], g["ja_nanoflann"], k, 2)
     assert O.max_rel_err(np.stack([v.cpu().numpy() for v in vals]), Wo, k).max() <= 1e-10
+
+
+def test_range_and_shards_equal_the_whole(ctx, torch_cuda):
+    T = torch_cuda
+    from rbf_b200 import shard
+    g = golden("square69_k21")
+    x, y = T.as_tensor(g["x"]).cuda(), T.as_tensor(g["y"]).cuda()
+    n, k = x.numel(), 21
+    d = R.make_desc(2)
+    full = [T.empty(n * k, dtype=T.float64, device="cuda") for _ in range(3)]
+    ja = T.as_tensor(g["ja_nanoflann"]).cuda()
+    ctx.assemble(d, x, y, k, ja, full)
+    parts_ja, parts_w = [], [[], [], []]
+    for rank in range(3):  # three "ranks" on one GPU, one after another
+        first, count, jr, vr = shard.assemble_shard(ctx, d, x, y, k, rank, 3)
+        parts_ja.append(jr)
+        for q in range(3):
+            parts_w[q].append(vr[q])
+    T.cuda.synchronize()
+    np.testing.assert_array_equal(T.cat(parts_ja).cpu().numpy(), g["ja_nanoflann"])
+    for q in range(3):
+        np.testing.assert_array_equal(T.cat(parts_w[q]).cpu().numpy(), full[q].cpu().numpy())
+
+
+def test_spmv_with_boundary_fix(ctx, torch_cuda):
+    T = torch_cuda
+    g = golden("shu_square_4786")
+    x, y = g["x"], g["y"]
+    n, k = x.size, 21
+    W, _ = O.assemble(x, y, g["ja_nanoflann"], k, 2)
+    u = np.sin(3 * x) * np.cos(2 * y)
+    bnd = np.flatnonzero(g["flag"]).astype(np.int32)
+    out = T.empty(n, dtype=T.float64, device="cuda")
+    ud = T.as_tensor(u).cuda()
+    jad = T.as_tensor(g["ja_nanoflann"]).cuda()
+    Wd = T.as_tensor(W[0]).cuda()
+    bd = T.as_tensor(bnd).cuda()
+    R.spmv(n, k, jad, Wd, ud, out, bd)
+    T.cuda.synchronize()
+    ref = O.spmv(g["ja_nanoflann"], W[0], u, k, bnd)
+    np.testing.assert_array_equal(out.cpu().numpy(), ref)  # same order, bit for bit
+    # and it is a Laplacian: -13 u in the interior up to the discretisation error
+    interior = np.setdiff1d(np.arange(n), bnd)
+    assert np.abs(ref[interior] + 13 * u[interior]).max() < 0.5
+
+
+def test_csr_batch_graph_replay(ctx, torch_cuda):
+    # on a non-default stream the batch is captured once, then replayed
+    T = torch_cuda
+    c = NS.config_disk_uneven(n=3000, nb=120, seed=17)
+    x, y, kvec, deg = c["x"], c["y"], c["kvec"], c["degree"]
+    n = x.size
+    kmax = int(kvec.max())
+    jaf = O.knn_brute(x, y, kmax).reshape(n, kmax)
+    ia = np.zeros(n + 1, np.int32)
+    ia[1:] = np.cumsum(kvec)
+    ja = np.concatenate([jaf[s, : kvec[s]] for s in range(n)]).astype(np.int32)
+    xd, yd = T.as_tensor(x).cuda(), T.as_tensor(y).cuda()
+    iad, jad, degd = T.as_tensor(ia).cuda(), T.as_tensor(ja).cuda(), T.as_tensor(deg).cuda()
+    vals = [T.empty(int(ia[-1]), dtype=T.float64, device="cuda") for _ in range(3)]
+    d = R.make_desc(2)
+    s = T.cuda.Stream()
+    outs, launches = [], []
+    for rep in range(3):
+        for v in vals:
+            v.fill_(np.nan)
+        l0 = ctx.launches()
+        with T.cuda.stream(s):
+            ctx.assemble_csr(d, xd, yd, iad, jad, vals, degree=degd, stream=s)
+        s.synchronize()
+        launches.append(ctx.launches() - l0)
+        outs.append(np.stack([v.cpu().numpy() for v in vals]))
+    assert launches[0] == launches[1] == launches[2] > 0
+    np.testing.assert_array_equal(outs[0], outs[1])
+    np.testing.assert_array_equal(outs[0], outs[2])
+    Wo, _ = O.assemble_csr(x, y, ia, ja, degree=deg, P=2, Q=0)
+    np.testing.assert_array_equal(outs[0], Wo)  # FP64 path: bit-identical to the oracle
