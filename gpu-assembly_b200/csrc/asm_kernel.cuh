@@ -109,9 +109,13 @@ struct AsmCfg {
     static_assert(NTP <= 128, "pivot keys carry the row index in 7 bits");
     // pivot row buffer: NTP columns, NRHS right-hand sides, the pivot's reciprocal
     static constexpr int BW = ((NTP + NRHS + 1 + VEC - 1) / VEC) * VEC;
-    // S row stride; odd (in 4-byte words per row pair) for the shared-memory
-    // elimination, whose lanes walk rows
-    static constexpr int LDS = SMEM ? NTP + 1 : NTP;
+    // S row stride. The lanes of a group read S down a column (the back
+    // substitution, the refinement sweeps, the shared-memory elimination) and
+    // write it across rows (the fill), so consecutive rows must start in
+    // different banks: an odd stride in elements for the shared-memory
+    // elimination; for the register path, whose rows move as 16-byte tuples,
+    // an odd stride in tuples (at most two rows of a column share a bank).
+    static constexpr int LDS = SMEM ? NTP + 1 : ((NTP / VEC) % 2 == 0 ? NTP + VEC : NTP);
     static constexpr int al16(int b) { return (b + 15) & ~15; }
     static constexpr int off_cx = 0;
     static constexpr int off_cy = off_cx + al16(8 * KMAX);
@@ -655,11 +659,24 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, char* sm
     // Column-oriented back substitution from S into X[c][q], a runtime loop:
     // the owner lane of step c's pivot row forms x_c = y * (1/pivot) and
     // broadcasts it by shuffle; rows pivoted before c update with S(r, c).
+    // The pivot row and the column of S of step c - 1 are loaded during step
+    // c, so only the select -> shuffle -> fma chain is serial.
     auto back_substitute = [&](T (&yy)[R][NRHS]) {
+        int pr = pivrow[NTP - 1];
+        T un[R];
+#pragma unroll
+        for (int sl = 0; sl < R; ++sl) un[sl] = S[(lr + GR * sl) * LDS + C::scol(NTP - 1)];
 #pragma unroll 1
         for (int c = NTP - 1; c >= 0; --c) {
-            const int pr = pivrow[c];
             const int osl = pr / GR, olane = (pr % GR) * GC;
+            T uc[R];
+#pragma unroll
+            for (int sl = 0; sl < R; ++sl) uc[sl] = un[sl];
+            const int cn = c > 0 ? c - 1 : 0;
+            pr = pivrow[cn];
+            const int scn = C::scol(cn);
+#pragma unroll
+            for (int sl = 0; sl < R; ++sl) un[sl] = S[(lr + GR * sl) * LDS + scn];
             T xq[NRHS];
             T dv = dinv[0];
 #pragma unroll
@@ -675,11 +692,9 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, char* sm
 #pragma unroll
                 for (int q = 0; q < NRHS; ++q) X[c * NRHS + q] = xq[q];
             }
-            const int sc = C::scol(c);
 #pragma unroll
             for (int sl = 0; sl < R; ++sl) {
-                const T u = S[(lr + GR * sl) * LDS + sc];
-                const T m = (pst[sl] < c) ? u : T(0);
+                const T m = (pst[sl] < c) ? uc[sl] : T(0);
 #pragma unroll
                 for (int q = 0; q < NRHS; ++q) yy[sl][q] = fma(-m, xq[q], yy[sl][q]);
             }
