@@ -86,6 +86,22 @@ struct AsmParams {
     int* work;  // dynamic work counter, or nullptr for a static stride
 };
 
+// Asynchronous global -> shared copies (cp.async, no register staging):
+// the next stencil's data is fetched while the current one is solved.
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(
+                     (unsigned)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(
+                     (unsigned)__cvta_generic_to_shared(dst)),
+                 "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 __device__ __forceinline__ unsigned group_mask(int G) {
     if (G == 32) return 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
@@ -127,7 +143,12 @@ struct AsmCfg {
     static constexpr int off_x64 = off_pm + (MIXED ? al16(8 * KMAX * NP) : 0);
     static constexpr int off_b64 = off_x64 + (MIXED ? al16(8 * NTP * NRHS) : 0);
     static constexpr int off_piv = off_b64 + (MIXED ? al16(8 * NTP * NRHS) : 0);
-    static constexpr int bytes = off_piv + al16(4 * NTP);  // row pivoted at each step
+    // next stencil, prefetched while this one is solved: its ja row, its
+    // centre (x, y) and its CSR bounds ia[s], ia[s + 1]
+    static constexpr int off_nja = off_piv + al16(4 * NTP);  // pivot row of each step before it
+    static constexpr int off_nxy = off_nja + al16(4 * KMAX);
+    static constexpr int off_nia = off_nxy + 16;
+    static constexpr int bytes = off_nia + 16;
     // S position of column c (de-interleaved by lane-column)
     static __device__ __forceinline__ int scol(int c) { return (c % GC) * CW + c / GC; }
 };
@@ -324,9 +345,10 @@ __device__ __forceinline__ void eliminate_smem(T* S, T* X, T* buf, int* pivrow, 
     __syncwarp(gmask);
 }
 
-template <typename T, int GR, int GC, int NTP, int NRHS, int P, int Q, bool MIXED, bool SMEM>
-__device__ __forceinline__ void assemble_one(const AsmParams& p, int s, char* smem, int lg,
-                                             unsigned gmask) {
+template <typename T, int GR, int GC, int NTP, int NRHS, int P, int Q, bool MIXED, bool SMEM,
+          bool PF>
+__device__ __forceinline__ void assemble_one(const AsmParams& p, int s, int sn, bool pre,
+                                             char* smem, int lg, unsigned gmask) {
     using C = AsmCfg<T, GR, GC, NTP, NRHS, P, Q, MIXED, SMEM>;
     constexpr int G = C::G, NP = C::NP, R = C::R, CW = C::CW, BW = C::BW, VEC = C::VEC;
     constexpr int LDS = C::LDS;
@@ -341,25 +363,62 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, char* sm
     double* b64 = reinterpret_cast<double*>(smem + C::off_b64);
 
     const int lr = lg / GC, lc = lg % GC;
-    const int off = p.ia ? p.ia[s] : (s - p.row_base) * p.k;
-    const int ks = p.ia ? p.ia[s + 1] - off : p.k;
+    int* nja = reinterpret_cast<int*>(smem + C::off_nja);
+    double* nxy = reinterpret_cast<double*>(smem + C::off_nxy);
+    int* nia = reinterpret_cast<int*>(smem + C::off_nia);
+
+    // Stencil s was prefetched (pre) by the previous call of this group: its
+    // neighbour coordinates wait in cx/cy (raw), its centre in nxy, its CSR
+    // bounds in nia. Otherwise everything comes from global memory.
+    int off, ks;
+    double x0, y0;
+    if (pre) {
+        cp_async_wait_all();
+        __syncwarp(gmask);
+        x0 = nxy[0];
+        y0 = nxy[1];
+        off = p.ia ? nia[0] : (s - p.row_base) * p.k;
+        ks = p.ia ? nia[1] - off : p.k;
+        __syncwarp(gmask);  // read before the slots are refilled below
+    } else {
+        x0 = p.x[s];
+        y0 = p.y[s];
+        off = p.ia ? p.ia[s] : (s - p.row_base) * p.k;
+        ks = p.ia ? p.ia[s + 1] - off : p.k;
+    }
     const int n = NP + ks;
+    // prefetch (PF), stage 1: the next stencil's centre and CSR bounds
+    if (PF && sn >= 0 && lg == 0) {
+        cp_async8(nxy, p.x + sn);
+        cp_async8(nxy + 1, p.y + sn);
+        if (p.ia) {
+            cp_async4(nia, p.ia + sn);
+            cp_async4(nia + 1, p.ia + sn + 1);
+        }
+    }
 
     // ---- gather + FP64 shift (+ minimum image), src/rbf_operators.h:354-358
     int e;
     {
         double gx[C::KPL], gy[C::KPL];
         int emax = -100000;
-        const double x0 = p.x[s], y0 = p.y[s];
 #pragma unroll
         for (int t = 0; t < C::KPL; ++t) {
             const int j = lg + t * G;
             gx[t] = 0.0;
             gy[t] = 0.0;
             if (j < ks) {
-                const int nb = __ldg(p.ja + off + j);
-                gx[t] = min_image(dsub(__ldg(p.x + nb), x0), p.Lx);
-                gy[t] = min_image(dsub(__ldg(p.y + nb), y0), p.Ly);
+                double xn, yn;
+                if (pre) {
+                    xn = cx[j];  // this lane's own prefetched slots
+                    yn = cy[j];
+                } else {
+                    const int nb = __ldg(p.ja + off + j);
+                    xn = __ldg(p.x + nb);
+                    yn = __ldg(p.y + nb);
+                }
+                gx[t] = min_image(dsub(xn, x0), p.Lx);
+                gy[t] = min_image(dsub(yn, y0), p.Ly);
                 if (gx[t] != 0.0) emax = max(emax, ilogb(fabs(gx[t])) + 1);
                 if (gy[t] != 0.0) emax = max(emax, ilogb(fabs(gy[t])) + 1);
             }
@@ -401,47 +460,73 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, char* sm
             }
         }
     }
-    // everything else, one row per lane
-    for (int r = lg; r < NTP; r += G) {
+    // node rows: monomials (the row and its transposed P^T column), the zero
+    // diagonal of the phi block, the right-hand sides
+    for (int i = lg; i < ks; i += G) {
+        const int r = NP + i;
         T* Sr = S + r * LDS;
-        if (r < NP) {
-            // P^T row: zero block, node columns written by the node rows below
-            for (int c = 0; c < NP; ++c) Sr[C::scol(c)] = T(0);
-            for (int c = n; c < NTP; ++c) Sr[C::scol(c)] = T(0);
+        const double xi = cx[i], yi = cy[i];
+        double mon[NP];
+        monomials<P>(xi, yi, mon);
 #pragma unroll
-            for (int q = 0; q < NRHS; ++q) {
-                const double v = q < p.nrhs ? rhs_poly<P>(p, q, r, e) : 0.0;
-                X[r * NRHS + q] = static_cast<T>(v);
-                if constexpr (MIXED) b64[r * NRHS + q] = v;
-            }
-        } else if (r < n) {
-            const int i = r - NP;
-            const double xi = cx[i], yi = cy[i];
-            double mon[NP];
-            monomials<P>(xi, yi, mon);
-#pragma unroll
-            for (int m = 0; m < NP; ++m) {
-                Sr[C::scol(m)] = static_cast<T>(mon[m]);
-                S[m * LDS + C::scol(r)] = static_cast<T>(mon[m]);
-                if constexpr (MIXED) pm[i * NP + m] = mon[m];
-            }
-            Sr[C::scol(r)] = T(0);
-            for (int c = n; c < NTP; ++c) Sr[C::scol(c)] = T(0);
-            double rv[NRHS];
-            rhs_node<P, Q, NRHS>(p, xi, yi, e, rv);
-#pragma unroll
-            for (int q = 0; q < NRHS; ++q) {
-                X[r * NRHS + q] = static_cast<T>(rv[q]);
-                if constexpr (MIXED) b64[r * NRHS + q] = rv[q];
-            }
-        } else {
-            for (int c = 0; c < NTP; ++c) Sr[C::scol(c)] = (c == r) ? T(1) : T(0);
-#pragma unroll
-            for (int q = 0; q < NRHS; ++q) {
-                X[r * NRHS + q] = T(0);
-                if constexpr (MIXED) b64[r * NRHS + q] = 0.0;
-            }
+        for (int m = 0; m < NP; ++m) {
+            Sr[C::scol(m)] = static_cast<T>(mon[m]);
+            S[m * LDS + C::scol(r)] = static_cast<T>(mon[m]);
+            if constexpr (MIXED) pm[i * NP + m] = mon[m];
         }
+        Sr[C::scol(r)] = T(0);
+        double rv[NRHS];
+        rhs_node<P, Q, NRHS>(p, xi, yi, e, rv);
+#pragma unroll
+        for (int q = 0; q < NRHS; ++q) {
+            X[r * NRHS + q] = static_cast<T>(rv[q]);
+            if constexpr (MIXED) b64[r * NRHS + q] = rv[q];
+        }
+    }
+    // P^T rows: right-hand sides (the polynomial reproduction conditions)
+    for (int r = lg; r < NP; r += G) {
+#pragma unroll
+        for (int q = 0; q < NRHS; ++q) {
+            const double v = q < p.nrhs ? rhs_poly<P>(p, q, r, e) : 0.0;
+            X[r * NRHS + q] = static_cast<T>(v);
+            if constexpr (MIXED) b64[r * NRHS + q] = v;
+        }
+    }
+    // padding rows: zero right-hand sides
+    for (int r = n + lg; r < NTP; r += G) {
+#pragma unroll
+        for (int q = 0; q < NRHS; ++q) {
+            X[r * NRHS + q] = T(0);
+            if constexpr (MIXED) b64[r * NRHS + q] = 0.0;
+        }
+    }
+    // the zero polynomial block, the padding columns of the real rows and the
+    // identity padding rows, each as a flat sequence over the lanes
+    for (int f = lg; f < NP * NP; f += G) S[(f / NP) * LDS + C::scol(f % NP)] = T(0);
+    for (int r = lg; r < n; r += G)
+        for (int c = n; c < NTP; ++c) S[r * LDS + C::scol(c)] = T(0);
+    for (int f = lg; f < (NTP - n) * NTP; f += G) {
+        const int r = n + f / NTP, c = f % NTP;
+        S[r * LDS + C::scol(c)] = (r == c) ? T(1) : T(0);
+    }
+    // prefetch, stage 2: the next stencil's ja row (its bounds have landed);
+    // its size goes to nia[2] (0: no next stencil), not held in a register
+    if constexpr (PF) {
+        int offn = 0, ksn = 0;
+        if (sn >= 0) {
+            if (p.ia) {
+                cp_async_wait_all();
+                __syncwarp(gmask);
+                offn = nia[0];
+                ksn = nia[1] - offn;
+            } else {
+                offn = (sn - p.row_base) * p.k;
+                ksn = p.k;
+            }
+            for (int j = lg; j < ksn; j += G) cp_async4(nja + j, p.ja + offn + j);
+        }
+        __syncwarp(gmask);  // every lane has read nia[0..1]
+        if (lg == 0) nia[2] = ksn;
     }
     __syncwarp(gmask);
 
@@ -701,6 +786,16 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, char* sm
         }
         __syncwarp(gmask);
     };
+    // prefetch, stage 3: the next stencil's neighbour coordinates into cx/cy
+    // (each lane gathers the slots j it fetched ja for, so no exchange)
+    if (const int ksn = PF ? nia[2] : 0; ksn > 0) {
+        cp_async_wait_all();
+        for (int j = lg; j < ksn; j += G) {
+            const int nb = nja[j];
+            cp_async8(cx + j, p.x + nb);
+            cp_async8(cy + j, p.y + nb);
+        }
+    }
     back_substitute(yv);
 
     const int nrhs = p.nrhs;
@@ -859,7 +954,7 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, char* sm
 }
 
 template <typename T, int GR, int GC, int NTP, int NRHS, int P, int Q, bool MIXED, int BLOCK,
-          int MINB, bool SMEM = false>
+          int MINB, bool SMEM = false, bool PF = true>
 __global__ void __launch_bounds__(BLOCK, MINB) asm_kernel(AsmParams p) {
     using C = AsmCfg<T, GR, GC, NTP, NRHS, P, Q, MIXED, SMEM>;
     constexpr int G = C::G;
@@ -872,23 +967,28 @@ __global__ void __launch_bounds__(BLOCK, MINB) asm_kernel(AsmParams p) {
     const int n = p.nitems_dev ? *p.nitems_dev : p.nitems;
     const int* list = (p.list && p.list_off_dev) ? p.list + *p.list_off_dev : p.list;
     const int ngroups = gridDim.x * GPB;
-    int it = blockIdx.x * GPB + gib;
-    if (p.work) {
+    auto claim = [&](int next_static) {
+        if (!p.work) return next_static;
         int v = 0;
         if (lg == 0) v = atomicAdd(p.work, 1);
-        it = __shfl_sync(gmask, v, 0, G);
-    }
-    // one call site: the stencil body is inlined once
+        return __shfl_sync(gmask, v, 0, G);
+    };
+    auto item = [&](int i) { return i < n ? (list ? list[i] : p.item_base + i) : -1; };
+    // One call site: the stencil body is inlined once. With PF each call
+    // also prefetches the next item's data (claimed one ahead), so every call
+    // but the first finds its stencil prefetched. The next item number waits
+    // in shared memory during the call (no register held across the solve).
+    int* next_it = reinterpret_cast<int*>(smem + C::off_nia) + 3;
+    int it = claim(blockIdx.x * GPB + gib);
+    bool pre = false;
     while (it < n) {
-        const int s = list ? list[it] : p.item_base + it;
-        assemble_one<T, GR, GC, NTP, NRHS, P, Q, MIXED, SMEM>(p, s, smem, lg, gmask);
-        if (p.work) {
-            int v = 0;
-            if (lg == 0) v = atomicAdd(p.work, 1);
-            it = __shfl_sync(gmask, v, 0, G);
-        } else {
-            it += ngroups;
-        }
+        const int itn = claim(it + ngroups);
+        if (lg == 0) *next_it = itn;
+        assemble_one<T, GR, GC, NTP, NRHS, P, Q, MIXED, SMEM, PF>(p, item(it), PF ? item(itn) : -1,
+                                                                  pre, smem, lg, gmask);
+        pre = PF;
+        it = *next_it;
+        __syncwarp(gmask);  // read before the next call overwrites it
     }
 }
 

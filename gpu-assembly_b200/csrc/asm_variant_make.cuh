@@ -10,15 +10,15 @@
 namespace rbfb {
 
 template <typename T, int GR, int GC, int NTP, int NRHS, int P, int Q, bool MIXED, int BLOCK,
-          int MINB, bool SMEM>
+          int MINB, bool SMEM, bool PF>
 Variant make_variant(const char* name) {
     using C = AsmCfg<T, GR, GC, NTP, NRHS, P, Q, MIXED, SMEM>;
     Variant v{};
     v.name = name;
     v.kernel =
-        reinterpret_cast<const void*>(&asm_kernel<T, GR, GC, NTP, NRHS, P, Q, MIXED, BLOCK, MINB, SMEM>);
+        reinterpret_cast<const void*>(&asm_kernel<T, GR, GC, NTP, NRHS, P, Q, MIXED, BLOCK, MINB, SMEM, PF>);
     v.launch = [](dim3 grid, int block, size_t smem, cudaStream_t st, const AsmParams& p) {
-        asm_kernel<T, GR, GC, NTP, NRHS, P, Q, MIXED, BLOCK, MINB, SMEM><<<grid, block, smem, st>>>(p);
+        asm_kernel<T, GR, GC, NTP, NRHS, P, Q, MIXED, BLOCK, MINB, SMEM, PF><<<grid, block, smem, st>>>(p);
     };
     v.mixed = MIXED;
     v.P = P;
@@ -34,9 +34,9 @@ Variant make_variant(const char* name) {
 
 }  // namespace rbfb
 
-#define RBFB_DEFINE_VARIANT(name, T, GR, GC, NTP, NRHS, P, Q, MIXED, BLOCK, MINB, SMEM)    \
-    namespace rbfb {                                                                       \
-    Variant variant_##name() {                                                             \
-        return make_variant<T, GR, GC, NTP, NRHS, P, Q, MIXED, BLOCK, MINB, SMEM>(#name);  \
-    }                                                                                      \
+#define RBFB_DEFINE_VARIANT(name, T, GR, GC, NTP, NRHS, P, Q, MIXED, BLOCK, MINB, SMEM, PF)    \
+    namespace rbfb {                                                                           \
+    Variant variant_##name() {                                                                 \
+        return make_variant<T, GR, GC, NTP, NRHS, P, Q, MIXED, BLOCK, MINB, SMEM, PF>(#name);  \
+    }                                                                                          \
     }
