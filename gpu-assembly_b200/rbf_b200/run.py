@@ -1,55 +1,155 @@
-"""Runs the hot path on one periodic jittered grid: k-NN stencils once, then
-the assembly `--reps` times in one precision. Prints one JSON line with the
-device time per assembly (CUDA events) and the call's counters.
+"""Runs the hot path on one of the benchmark workloads: k-NN stencils once,
+then the assembly `--reps` times in each requested form. Prints one JSON line
+with the device time per assembly (CUDA events), stencils/s and the call's
+counters; with both forms, the mixed form's max relative weight error
+against the FP64 form (which is bit-identical to the CPU restatement of the
+reference's assembly, as the parity tests establish).
 
     python -m rbf_b200.run --grid 256 --precision mixed --reps 3
+    python -m rbf_b200.run --workload disk --precision both
+    python -m rbf_b200.run --workload bump --precision both
 
-Used to profile a single kernel shape on a small case (e.g. under ncu with
-``-k regex:asm_kernel``); the workload is the benchmark's at a smaller size.
+Workloads:
+  periodic  jittered m x m grid in the periodic unit square (m = --grid),
+            k=35, PHS r^5 + degree 3, fixed-width stencils
+  disk      4,194,304 nodes on the unit disk, 8,192 boundary nodes with
+            k in [48, 64] at degree 4, interior k in {21, 28, 35} at degree
+            2/3: ragged CSR stencils, bucketed by system size, graph-replayed
+  bump      2,097,152 nodes with a 4x Gaussian-bump density, k=64, PHS r^7 +
+            degree 4 (n=79)
+The single-kernel shapes are also what the profiles are captured on (e.g.
+under ncu with ``-k regex:asm_kernel`` on ``--grid 512``).
 """
 from __future__ import annotations
 
 import argparse
 import json
 
+import numpy as np
 import torch
 
 import rbf_b200 as R
 from rbf_b200 import nodesets as NS
 
 
+def _events_ms(fn, reps, stream):
+    """Device time of fn(stats=False) on `stream` (CUDA events, after one
+    warm-up call that also fills autotune caches and captures graphs), then
+    one call with stats for the counters."""
+    ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    fn(False)
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(reps):
+        ea.record(stream)
+        fn(False)
+        eb.record(stream)
+        torch.cuda.synchronize()
+        ms.append(ea.elapsed_time(eb))
+    return ms, fn(True)
+
+
+def _max_rel_err(a, b, ia):
+    """Per-stencil max |a - b| / max |b|, worst over stencils and right-hand
+    sides (rows of ragged width given by ia)."""
+    worst = 0.0
+    seg = torch.repeat_interleave(torch.arange(ia.numel() - 1, device=ia.device),
+                                  (ia[1:] - ia[:-1]).long())
+    n = ia.numel() - 1
+    for va, vb in zip(a, b):
+        num = torch.zeros(n, dtype=torch.float64, device=va.device)
+        den = torch.zeros(n, dtype=torch.float64, device=va.device)
+        num.scatter_reduce_(0, seg, (va - vb).abs(), reduce="amax")
+        den.scatter_reduce_(0, seg, vb.abs(), reduce="amax")
+        worst = max(worst, float((num / den.clamp_min(1e-300)).max()))
+    return worst
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--grid", type=int, default=256)
+    ap.add_argument("--workload", choices=["periodic", "disk", "bump"], default="periodic")
+    ap.add_argument("--grid", type=int, default=256, help="periodic: grid side")
+    ap.add_argument("--n", type=int, default=None, help="disk/bump: number of nodes")
     ap.add_argument("--k", type=int, default=35)
     ap.add_argument("--degree", type=int, default=3)
-    ap.add_argument("--precision", choices=["fp64", "mixed"], default="mixed")
+    ap.add_argument("--precision", choices=["fp64", "mixed", "both"], default="mixed")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--tune", action="store_true", help="autotune the shape first")
     a = ap.parse_args(argv)
-    x, y, _ = NS.jittered_grid(a.grid, 0.3, seed=2, periodic=True)
-    n, k = x.size, a.k
     dev = torch.device("cuda", 0)
-    xd, yd = torch.as_tensor(x, device=dev), torch.as_tensor(y, device=dev)
-    ja = torch.empty(n * k, dtype=torch.int32, device=dev)
-    vals = [torch.empty(n * k, dtype=torch.float64, device=dev) for _ in range(3)]
-    info = torch.empty(n, dtype=torch.int32, device=dev)
-    per = (1.0, 1.0)
-    prec = R.FP64 if a.precision == "fp64" else R.FP32_IR
-    d = R.make_desc(a.degree, 0, R.DEFAULT_OPS, prec, True, period=per)
+    stream = torch.cuda.Stream(dev)  # non-default: the CSR path replays a CUDA graph on it
+    forms = ["fp64", "mixed"] if a.precision == "both" else [a.precision]
+    prec = {"fp64": R.FP64, "mixed": R.FP32_IR}
+    out = {"workload": a.workload}
+
     with R.Context(0) as ctx:
-        ctx.knn_stencils(xd, yd, k, ja, period=per)
-        shape = None
-        if a.tune:
-            shape = R.variant_name(ctx.autotune(d, xd, yd, k, ja, vals))
-        ms = []
-        st = None
-        for _ in range(a.reps):
-            st = ctx.assemble(d, xd, yd, k, ja, vals, info, stats=True)
-            ms.append(st["ms"])
+        if a.workload == "disk":
+            c = NS.config_disk_uneven(**({"n": a.n} if a.n else {}))
+            x, y = c["x"], c["y"]
+            n = x.size
+            xd, yd = torch.as_tensor(x, device=dev), torch.as_tensor(y, device=dev)
+            kvec = torch.as_tensor(c["kvec"], device=dev)
+            deg = torch.as_tensor(c["degree"], device=dev)
+            kmax = int(kvec.max())
+            jaf = torch.empty(n * kmax, dtype=torch.int32, device=dev)
+            ctx.knn_stencils(xd, yd, kmax, jaf)
+            keep = torch.arange(kmax, device=dev)[None, :] < kvec[:, None]
+            ja = jaf.view(n, kmax)[keep].contiguous()
+            ia = torch.zeros(n + 1, dtype=torch.int32, device=dev)
+            ia[1:] = torch.cumsum(kvec, 0).to(torch.int32)
+            del jaf
+            nnz = int(ia[-1])
+            torch.cuda.synchronize()
+            res = {}
+            for f in forms:
+                vals = [torch.empty(nnz, dtype=torch.float64, device=dev) for _ in range(3)]
+                info = torch.empty(n, dtype=torch.int32, device=dev)
+                d = R.make_desc(3, 0, R.DEFAULT_OPS, prec[f], True)
+                ms, st = _events_ms(lambda sts: ctx.assemble_csr(d, xd, yd, ia, ja, vals, degree=deg,
+                                                                 info=info, stats=sts,
+                                                                 stream=stream),
+                                    a.reps, stream)
+                res[f] = vals
+                out[f] = {"ms": ms, "stencils_per_s": n / (min(ms) * 1e-3), "stats": st,
+                          "bad_info": int((info != 0).sum())}
+            out.update(stencils=n, nnz=nnz, k_range=[int(kvec.min()), kmax],
+                       degrees=sorted(set(int(v) for v in np.unique(c["degree"]))))
+            if len(forms) == 2:
+                out["mixed_max_rel_err_vs_fp64"] = _max_rel_err(res["mixed"], res["fp64"], ia)
+        else:
+            if a.workload == "bump":
+                c = NS.config_bump(**({"n": a.n} if a.n else {}))
+                x, y = c["x"], c["y"]
+                k, P, per = c["k"], c["P"], None
+            else:
+                x, y, _ = NS.jittered_grid(a.grid, 0.3, seed=2, periodic=True)
+                k, P, per = a.k, a.degree, (1.0, 1.0)
+            n = x.size
+            xd, yd = torch.as_tensor(x, device=dev), torch.as_tensor(y, device=dev)
+            ja = torch.empty(n * k, dtype=torch.int32, device=dev)
+            ctx.knn_stencils(xd, yd, k, ja, period=per)
+            torch.cuda.synchronize()
+            res = {}
+            shape = None
+            for f in forms:
+                vals = [torch.empty(n * k, dtype=torch.float64, device=dev) for _ in range(3)]
+                info = torch.empty(n, dtype=torch.int32, device=dev)
+                d = R.make_desc(P, 0, R.DEFAULT_OPS, prec[f], True, period=per)
+                if a.tune:
+                    shape = R.variant_name(ctx.autotune(d, xd, yd, k, ja, vals))
+                ms, st = _events_ms(lambda sts: ctx.assemble(d, xd, yd, k, ja, vals, info, stats=sts,
+                                                             stream=stream), a.reps, stream)
+                res[f] = vals
+                out[f] = {"ms": ms, "stencils_per_s": n / (min(ms) * 1e-3), "stats": st,
+                          "bad_info": int((info != 0).sum()), "shape": shape}
+            out.update(stencils=n, k=k, degree=P)
+            if a.workload == "periodic":
+                out["grid"] = a.grid
+            if len(forms) == 2:
+                ia = torch.arange(0, (n + 1) * k, k, dtype=torch.int32, device=dev)
+                out["mixed_max_rel_err_vs_fp64"] = _max_rel_err(res["mixed"], res["fp64"], ia)
         torch.cuda.synchronize()
-        print(json.dumps({"grid": a.grid, "stencils": n, "precision": a.precision,
-                          "shape": shape, "ms": ms, "stats": st}))
+    print(json.dumps(out))
 
 
 if __name__ == "__main__":
