@@ -345,10 +345,43 @@ __device__ __forceinline__ void eliminate_smem(T* S, T* X, T* buf, int* pivrow, 
     __syncwarp(gmask);
 }
 
+// The prefetch of a group's first stencil, done up front (the stages that
+// assemble_one spreads over a stencil's solve, back to back): centre and CSR
+// bounds, then the ja row, then the neighbour coordinates into cx/cy.
+template <class C>
+__device__ __forceinline__ void prefetch_first(const AsmParams& p, int s, char* smem, int lg,
+                                               unsigned gmask) {
+    constexpr int G = C::G;
+    double* cx = reinterpret_cast<double*>(smem + C::off_cx);
+    double* cy = reinterpret_cast<double*>(smem + C::off_cy);
+    int* nja = reinterpret_cast<int*>(smem + C::off_nja);
+    double* nxy = reinterpret_cast<double*>(smem + C::off_nxy);
+    int* nia = reinterpret_cast<int*>(smem + C::off_nia);
+    if (lg == 0) {
+        cp_async8(nxy, p.x + s);
+        cp_async8(nxy + 1, p.y + s);
+        if (p.ia) {
+            cp_async4(nia, p.ia + s);
+            cp_async4(nia + 1, p.ia + s + 1);
+        }
+    }
+    cp_async_wait_all();
+    __syncwarp(gmask);
+    const int off = p.ia ? nia[0] : (s - p.row_base) * p.k;
+    const int ks = p.ia ? nia[1] - off : p.k;
+    for (int j = lg; j < ks; j += G) cp_async4(nja + j, p.ja + off + j);
+    cp_async_wait_all();
+    for (int j = lg; j < ks; j += G) {  // this lane's own ja slots
+        const int nb = nja[j];
+        cp_async8(cx + j, p.x + nb);
+        cp_async8(cy + j, p.y + nb);
+    }
+}
+
 template <typename T, int GR, int GC, int NTP, int NRHS, int P, int Q, bool MIXED, bool SMEM,
           bool PF>
-__device__ __forceinline__ void assemble_one(const AsmParams& p, int s, int sn, bool pre,
-                                             char* smem, int lg, unsigned gmask) {
+__device__ __forceinline__ void assemble_one(const AsmParams& p, int s, int sn, char* smem,
+                                             int lg, unsigned gmask) {
     using C = AsmCfg<T, GR, GC, NTP, NRHS, P, Q, MIXED, SMEM>;
     constexpr int G = C::G, NP = C::NP, R = C::R, CW = C::CW, BW = C::BW, VEC = C::VEC;
     constexpr int LDS = C::LDS;
@@ -367,12 +400,14 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, int sn, 
     double* nxy = reinterpret_cast<double*>(smem + C::off_nxy);
     int* nia = reinterpret_cast<int*>(smem + C::off_nia);
 
-    // Stencil s was prefetched (pre) by the previous call of this group: its
-    // neighbour coordinates wait in cx/cy (raw), its centre in nxy, its CSR
-    // bounds in nia. Otherwise everything comes from global memory.
+    // With PF, stencil s was prefetched (by the previous call of this group,
+    // or by prefetch_first): its neighbour coordinates wait in cx/cy (raw),
+    // its centre in nxy, its CSR bounds in nia. Without PF everything comes
+    // from global memory. (Every call of a shape takes the same branch, so
+    // the stencil body exists once in the kernel's code.)
     int off, ks;
     double x0, y0;
-    if (pre) {
+    if constexpr (PF) {
         cp_async_wait_all();
         __syncwarp(gmask);
         x0 = nxy[0];
@@ -409,7 +444,7 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, int sn, 
             gy[t] = 0.0;
             if (j < ks) {
                 double xn, yn;
-                if (pre) {
+                if constexpr (PF) {
                     xn = cx[j];  // this lane's own prefetched slots
                     yn = cy[j];
                 } else {
@@ -975,18 +1010,20 @@ __global__ void __launch_bounds__(BLOCK, MINB) asm_kernel(AsmParams p) {
     };
     auto item = [&](int i) { return i < n ? (list ? list[i] : p.item_base + i) : -1; };
     // One call site: the stencil body is inlined once. With PF each call
-    // also prefetches the next item's data (claimed one ahead), so every call
-    // but the first finds its stencil prefetched. The next item number waits
-    // in shared memory during the call (no register held across the solve).
+    // also prefetches the next item's data (claimed one ahead) and the first
+    // item is prefetched before the loop, so every call finds its stencil
+    // prefetched. The next item number waits in shared memory during the
+    // call (no register held across the solve).
     int* next_it = reinterpret_cast<int*>(smem + C::off_nia) + 3;
     int it = claim(blockIdx.x * GPB + gib);
-    bool pre = false;
+    if constexpr (PF) {
+        if (it < n) prefetch_first<C>(p, item(it), smem, lg, gmask);
+    }
     while (it < n) {
         const int itn = claim(it + ngroups);
         if (lg == 0) *next_it = itn;
         assemble_one<T, GR, GC, NTP, NRHS, P, Q, MIXED, SMEM, PF>(p, item(it), PF ? item(itn) : -1,
-                                                                  pre, smem, lg, gmask);
-        pre = PF;
+                                                                  smem, lg, gmask);
         it = *next_it;
         __syncwarp(gmask);  // read before the next call overwrites it
     }
