@@ -30,6 +30,7 @@ LIB_PATH = PKG / "lib" / "librbf_b200.so"
 OK, EINVAL, ECUDA, ENOMEM, EUNSUPPORTED, ETIMEOUT, EBUDGET, ENOTFOUND, EBUSY, ETOOBIG = (
     0, -1, -2, -3, -4, -5, -6, -7, -8, -9)
 STATIC_MAX_NODES = 65536  # limit of rbfb_knn_stencils_static
+MORTON, HILBERT = 0, 1  # curves of rbfb_curve_keys / rbfb_curve_order
 OP_INTERP, OP_LAPLACE, OP_DX, OP_DY, OP_DXX, OP_DYY, OP_DXY = 1, 2, 4, 8, 16, 32, 64
 FP64, FP32_IR = 0, 1
 MAX_RHS = 8
@@ -99,6 +100,12 @@ _PROTOS = {
     "rbfb_fill_matrices": (_i, [_vp, C.POINTER(Desc), _i, _vp, _vp, _vp, _vp, _vp, _i, _vp]),
     "rbfb_store_to_csr": (_i, [_i, _vp, _vp, _vp, _vp, _vp]),
     "rbfb_spmv": (_i, [_i, _i, _vp, _vp, _vp, _vp, _vp, _i, _vp]),
+    "rbfb_curve_keys": (_i, [_vp, _i, _vp, _vp, _vp, _i, _i, _vp, _vp]),
+    "rbfb_curve_order": (_i, [_vp, _i, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp]),
+    "rbfb_boundary_last": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
+    "rbfb_renumber_stencils": (_i, [_i, _i, _vp, _vp, _vp, _vp, _vp]),
+    "rbfb_renumber_csr": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "rbfb_permute": (_i, [_i, _vp, _vp, _vp, _i, _vp]),
     "rbfb_solve_dp": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "rbfb_autotune": (_i, [_vp, C.POINTER(Desc), _i, _vp, _vp, _i, _vp, _vp]),
     "rbfb_variant_name": (C.c_char_p, [_i]),
@@ -303,6 +310,32 @@ class Context:
                                  _ptr(ja), tab)
         return self._check(st, "autotune")
 
+    # ---- node renumbering (permutations in gather form: perm[new] = old)
+    def curve_keys(self, x, y, keys, ndiv=16, curve=MORTON, bbox=None, stream=None):
+        """int64 device keys <- Morton (curve=MORTON) or Hilbert curve keys."""
+        bb = None if bbox is None else (C.c_double * 4)(*bbox)
+        st = lib().rbfb_curve_keys(self.h, x.numel(), _ptr(x), _ptr(y), bb, ndiv, curve,
+                                   _ptr(keys), _stream(stream))
+        return self._check(st, "curve_keys")
+
+    def curve_order(self, x, y, perm, inv=None, keys=None, ndiv=16, curve=MORTON, bbox=None,
+                    stream=None):
+        """perm (int32 device) <- the nodes in stable curve order."""
+        bb = None if bbox is None else (C.c_double * 4)(*bbox)
+        st = lib().rbfb_curve_order(self.h, x.numel(), _ptr(x), _ptr(y), bb, ndiv, curve,
+                                    _ptr(keys), _ptr(perm), _ptr(inv), _stream(stream))
+        return self._check(st, "curve_order")
+
+    def boundary_last(self, flag, perm, inv=None, stream=None):
+        st = lib().rbfb_boundary_last(self.h, flag.numel(), _ptr(flag), _ptr(perm), _ptr(inv),
+                                      _stream(stream))
+        return self._check(st, "boundary_last")
+
+    def renumber_csr(self, ia, ja, perm, inv, ia_out, ja_out, stream=None):
+        st = lib().rbfb_renumber_csr(self.h, perm.numel(), _ptr(ia), _ptr(ja), _ptr(perm),
+                                     _ptr(inv), _ptr(ia_out), _ptr(ja_out), _stream(stream))
+        return self._check(st, "renumber_csr")
+
 
 def knn_stencils_static(x, y, k, ja, period=None, stream=None):
     """rbfb_knn_stencils_static: the k-NN search without any allocation
@@ -317,6 +350,22 @@ def knn_stencils_static(x, y, k, ja, period=None, stream=None):
 def variant_name(index: int):
     v = lib().rbfb_variant_name(index)
     return None if v is None else v.decode()
+
+
+def renumber_stencils(n, k, ja, perm, inv, ja_out, stream=None):
+    """ja_out[s*k+j] = inv[ja[perm[s]*k+j]] (out of place)."""
+    st = lib().rbfb_renumber_stencils(n, k, _ptr(ja), _ptr(perm), _ptr(inv), _ptr(ja_out),
+                                      _stream(stream))
+    if st != OK:
+        raise RbfError(st, "renumber_stencils")
+
+
+def permute(perm, src, out, stream=None):
+    """out[i] = src[perm[i]] for 4- or 8-byte elements (out of place)."""
+    st = lib().rbfb_permute(perm.numel(), _ptr(perm), _ptr(src), _ptr(out), src.element_size(),
+                            _stream(stream))
+    if st != OK:
+        raise RbfError(st, "permute")
 
 
 def spmv(n, k, ja, values, u, out, bnd=None, stream=None):

@@ -225,6 +225,40 @@ int rbfb_solve_dp(double* A, int* ipiv, double* B, int* info, void* stream);
 int rbfb_spmv(int n, int k, const int* ja, const double* values, const double* u, double* out,
               const int* bnd, int nbnd, void* stream);
 
+/* ---- node renumbering (locality) ------------------------------------------
+ * A permutation is stored in gather form, as the reference's
+ * rbf::Permutation (src/rbf_reorder.h:68-80): perm[i] is the OLD index of
+ * the node at NEW position i; inv (old -> new) is optional everywhere. */
+
+/* Space-filling-curve keys: curve 0 = Morton (Z order), 1 = Hilbert; ndiv
+ * levels in 1..31 give 2*ndiv key bits. bbox_h is a HOST double[4] {xmin,
+ * ymin, xmax, ymax} (the layout of rbf::BBox2<double>), or NULL for the
+ * nodes' own bounding box. rbf_morton_keys / rbf_hilbert_keys with zidx /
+ * hidx (src/rbf_ordering.F90:31-63,82-218; src/rbf_reorder.h:196-208). */
+int rbfb_curve_keys(rbfb_ctx* ctx, int n, const double* x, const double* y, const double* bbox_h,
+                    int ndiv, int curve, int64_t* keys, void* stream);
+/* The nodes in curve order, stable (equal keys keep node order): morton_order
+ * / hilbert_order (src/rbf_reorder.h:210-230). perm is required; keys (the
+ * sorted keys) and inv may be NULL. */
+int rbfb_curve_order(rbfb_ctx* ctx, int n, const double* x, const double* y, const double* bbox_h,
+                     int ndiv, int curve, int64_t* keys, int* perm, int* inv, void* stream);
+/* Nodes with nonzero flag last, both groups keeping their order:
+ * boundary_last_by_flag (src/rbf_reorder.h:232-244). */
+int rbfb_boundary_last(rbfb_ctx* ctx, int n, const int* flag, int* perm, int* inv, void* stream);
+/* A' = P A P^T of a fixed-width stencil table: ja_out[s*k+j] =
+ * inv[ja[perm[s]*k+j]] (renumber_stencils, src/rbf_reorder.h:256-281; here
+ * out of place: ja_out must not alias ja). Self-first rows stay self-first. */
+int rbfb_renumber_stencils(int n, int k, const int* ja, const int* perm, const int* inv,
+                           int* ja_out, void* stream);
+/* The same for CSR stencils (renumber_csr, src/rbf_reorder.h:283-303):
+ * ia_out has n+1 entries; out of place. */
+int rbfb_renumber_csr(rbfb_ctx* ctx, int n, const int* ia, const int* ja, const int* perm,
+                      const int* inv, int* ia_out, int* ja_out, void* stream);
+/* Node data into the new numbering: out[i] = in[perm[i]] for 4- or 8-byte
+ * elements (Permutation::permute, src/rbf_reorder.h:68-80; out of place).
+ * Also composes permutations: permuting p by q gives "p, then q". */
+int rbfb_permute(int n, const int* perm, const void* in, void* out, int elem_bytes, void* stream);
+
 /* ---- tuning --------------------------------------------------------------- */
 /* Times the compiled kernel shapes for one system size and precision on the
  * given workload and records the fastest in the context's launch table

@@ -67,6 +67,17 @@ def lib():
                                             C.c_void_p]
         L.orc_spmv.restype = None
         L.orc_spmv.argtypes = [C.c_int, C.c_int, _ip, _dp, _dp, _dp, C.c_void_p, C.c_int]
+        L.orc_curve_keys.restype = C.c_int
+        L.orc_curve_keys.argtypes = [C.c_int, _dp, _dp, C.c_void_p, C.c_int, C.c_int,
+                                     np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")]
+        L.orc_curve_order.restype = C.c_int
+        L.orc_curve_order.argtypes = [C.c_int, _dp, _dp, C.c_void_p, C.c_int, C.c_int, _ip]
+        L.orc_boundary_last.restype = None
+        L.orc_boundary_last.argtypes = [C.c_int, _ip, _ip]
+        L.orc_renumber_stencils.restype = None
+        L.orc_renumber_stencils.argtypes = [C.c_int, C.c_int, _ip, _ip, _ip]
+        L.orc_renumber_csr.restype = None
+        L.orc_renumber_csr.argtypes = [C.c_int, _ip, _ip, _ip, _ip, _ip]
         L.orc_phs.restype = C.c_double
         L.orc_phs.argtypes = [C.c_int, C.c_double]
         L.orc_set_threads.argtypes = [C.c_int]
@@ -276,6 +287,51 @@ def spmv(ja, values, u, k, bnd=None):
     lib().orc_spmv(n, k, ja, values, u, out, None if b is None else b.ctypes.data,
                    0 if b is None else b.size)
     return out
+
+
+MORTON, HILBERT = 0, 1
+
+
+def curve_keys(x, y, ndiv=16, curve=MORTON, bbox=None):
+    """zidx / hidx keys of every point (int64)."""
+    x, y = _f64(x), _f64(y)
+    keys = np.empty(x.size, np.int64)
+    bb = None if bbox is None else (C.c_double * 4)(*bbox)
+    if lib().orc_curve_keys(x.size, x, y, bb, ndiv, curve, keys) < 0:
+        raise ValueError("bad ndiv or curve")
+    return keys
+
+
+def curve_order(x, y, ndiv=16, curve=MORTON, bbox=None):
+    """morton_order / hilbert_order: perm[new] = old (stable)."""
+    x, y = _f64(x), _f64(y)
+    perm = np.empty(x.size, np.int32)
+    bb = None if bbox is None else (C.c_double * 4)(*bbox)
+    if lib().orc_curve_order(x.size, x, y, bb, ndiv, curve, perm) < 0:
+        raise ValueError("bad ndiv or curve")
+    return perm
+
+
+def boundary_last(flag):
+    flag = _i32(flag)
+    perm = np.empty(flag.size, np.int32)
+    lib().orc_boundary_last(flag.size, flag, perm)
+    return perm
+
+
+def renumber_stencils(ja, k, perm):
+    ja, perm = _i32(ja), _i32(perm)
+    out = np.empty_like(ja)
+    lib().orc_renumber_stencils(perm.size, k, ja, perm, out)
+    return out
+
+
+def renumber_csr(ia, ja, perm):
+    ia, ja, perm = _i32(ia), _i32(ja), _i32(perm)
+    ia_out = np.empty_like(ia)
+    ja_out = np.empty_like(ja)
+    lib().orc_renumber_csr(perm.size, ia, ja, perm, ia_out, ja_out)
+    return ia_out, ja_out
 
 
 def max_rel_err(w, w_ref, k):

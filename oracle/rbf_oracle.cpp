@@ -16,6 +16,10 @@
 //   brute k-NN       test_spatial brute_knn + metric  test/test_spatial.cpp:59-82
 //                    nanoflann L2_Simple_Adaptor    third_party/nanoflann/nanoflann.hpp:690-699
 //                    ckdtree wrap_distance          third_party/ckdtree/src/distance.h:262-272
+//   curve keys       zidx / hidx                    src/rbf_ordering.F90:82-218
+//   curve order      morton_order / hilbert_order   src/rbf_reorder.h:180-185,210-230
+//   boundary last    boundary_last_by_flag          src/rbf_reorder.h:232-244
+//   renumbering      renumber_stencils / _csr       src/rbf_reorder.h:256-303
 //
 // What it adds, because the reference has it only as intent:
 //   * derivative right-hand sides at the stencil centre (Laplacian, d/dx,
@@ -681,4 +685,93 @@ extern "C" void orc_spmv(int n, int k, const int* ja, const double* values, cons
         out[s] = acc;
     }
     for (int b = 0; b < nbnd; ++b) out[bnd[b]] = u[bnd[b]];
+}
+
+// ---- node renumbering ------------------------------------------------------------
+// Curve keys as zidx / hidx compute them (src/rbf_ordering.F90:82-218): at
+// each of ndiv levels the key shifts by two bits, the quadrant q of the
+// point against the box midpoint cx = x0 + 0.5 * (x1 - x0) (each operation
+// rounded) is added (Morton) or mapped through the Hilbert state tables
+// (table(q, rot), tr(q, rot)), and the box shrinks to that quadrant. bbox is
+// {xmin, ymin, xmax, ymax}, NULL for the points' own (compute_bbox,
+// src/rbf_reorder.h:60-66). curve 0 = Morton, 1 = Hilbert.
+extern "C" int orc_curve_keys(int n, const double* x, const double* y, const double* bbox, int ndiv,
+                              int curve, long long* keys) {
+    if (n < 0 || ndiv < 1 || ndiv > 31 || (curve != 0 && curve != 1)) return -1;
+    if (n == 0) return 0;
+    double bb[4];
+    if (bbox) {
+        for (int i = 0; i < 4; ++i) bb[i] = bbox[i];
+    } else {
+        bb[0] = *std::min_element(x, x + n);
+        bb[1] = *std::min_element(y, y + n);
+        bb[2] = *std::max_element(x, x + n);
+        bb[3] = *std::max_element(y, y + n);
+    }
+    // hidx's table(q, rot) and tr(q, rot), as [rot][q]
+    static const int hdigit[4][4] = {{0, 3, 1, 2}, {2, 3, 1, 0}, {2, 1, 3, 0}, {0, 1, 3, 2}};
+    static const int hnext[4][4] = {{3, 1, 0, 0}, {1, 0, 1, 2}, {2, 2, 3, 1}, {0, 3, 2, 3}};
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        double x0 = bb[0], y0 = bb[1], x1 = bb[2], y1 = bb[3];
+        long long z = 0;
+        int rot = 0;
+        for (int l = 0; l < ndiv; ++l) {
+            z <<= 2;
+            const double cx = x0 + 0.5 * (x1 - x0);
+            const double cy = y0 + 0.5 * (y1 - y0);
+            const int q = (x[i] > cx ? 1 : 0) + (y[i] > cy ? 2 : 0);
+            if (curve == 0) {
+                z += q;
+            } else {
+                z += hdigit[rot][q];
+                rot = hnext[rot][q];
+            }
+            if (x[i] > cx) x0 = cx; else x1 = cx;
+            if (y[i] > cy) y0 = cy; else y1 = cy;
+        }
+        keys[i] = z;
+    }
+    return 0;
+}
+
+// morton_order / hilbert_order: indices stably sorted by key (order_by_keys,
+// src/rbf_reorder.h:180-185). perm[i] = old index at new position i.
+extern "C" int orc_curve_order(int n, const double* x, const double* y, const double* bbox,
+                               int ndiv, int curve, int* perm) {
+    std::vector<long long> keys(static_cast<size_t>(std::max(n, 0)));
+    if (orc_curve_keys(n, x, y, bbox, ndiv, curve, keys.data()) < 0) return -1;
+    for (int i = 0; i < n; ++i) perm[i] = i;
+    std::stable_sort(perm, perm + n, [&keys](int a, int b) { return keys[a] < keys[b]; });
+    return 0;
+}
+
+// boundary_last_by_flag (src/rbf_reorder.h:232-244): stable partition,
+// nonzero flag last.
+extern "C" void orc_boundary_last(int n, const int* flag, int* perm) {
+    for (int i = 0; i < n; ++i) perm[i] = i;
+    std::stable_partition(perm, perm + n, [flag](int i) { return flag[i] == 0; });
+}
+
+// renumber_stencils (src/rbf_reorder.h:272-281), out of place:
+// out[s*k+j] = inv[ja[perm[s]*k+j]].
+extern "C" void orc_renumber_stencils(int n, int k, const int* ja, const int* perm, int* out) {
+    std::vector<int> inv(static_cast<size_t>(n));
+    for (int i = 0; i < n; ++i) inv[perm[i]] = i;
+    for (int s = 0; s < n; ++s)
+        for (int j = 0; j < k; ++j)
+            out[static_cast<size_t>(s) * k + j] = inv[ja[static_cast<size_t>(perm[s]) * k + j]];
+}
+
+// renumber_csr (src/rbf_reorder.h:286-303), out of place.
+extern "C" void orc_renumber_csr(int n, const int* ia, const int* ja, const int* perm, int* ia_out,
+                                 int* ja_out) {
+    std::vector<int> inv(static_cast<size_t>(n));
+    for (int i = 0; i < n; ++i) inv[perm[i]] = i;
+    ia_out[0] = 0;
+    for (int i = 0; i < n; ++i) {
+        const int a = ia[perm[i]], b = ia[perm[i] + 1];
+        for (int t = a; t < b; ++t) ja_out[ia_out[i] + (t - a)] = inv[ja[t]];
+        ia_out[i + 1] = ia_out[i] + (b - a);
+    }
 }
