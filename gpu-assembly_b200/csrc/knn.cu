@@ -31,6 +31,7 @@
 #include <cmath>
 #include <cstdint>
 #include <mutex>
+#include <type_traits>
 
 #include "asm_math.cuh"
 #include "runtime.h"
@@ -294,6 +295,12 @@ __global__ void __launch_bounds__(kWarps * 32) query_kernel(QueryArgs a) {
             }
             double bound = fmin(bx, by);
             bound = bound * (1.0 - 1e-9) - 1e-15 * fmax(fabs(qx), fabs(qy));
+            // Only candidates inside the circle of radius `bound` (inscribed in
+            // the searched block) are kept: when at least k of them are found,
+            // the k nearest nodes are among them, since every node outside is
+            // farther than all of these; otherwise the block grows. (A block
+            // that covers the whole domain keeps everything.)
+            const double bound2 = bound >= 1e299 ? INFINITY : (bound > 0.0 ? bound * bound : 0.0);
             // gather candidates chunk by chunk; the current best k stay at the front
             int have = 0;  // entries in the buffer (best-so-far first)
             int total = 0;
@@ -321,12 +328,13 @@ __global__ void __launch_bounds__(kWarps * 32) query_kernel(QueryArgs a) {
                     const int beg = a.start[cyy * g.cx + c0], end = a.start[cyy * g.cx + c1 + 1];
                     for (int base = beg; base < end; base += 32) {
                         const int j = base + lane;
-                        const bool ok = j < end;
+                        bool ok = j < end;
                         unsigned long long dk = 0;
                         int ik = 0;
                         if (ok) {
-                            dk = (unsigned long long)__double_as_longlong(
-                                sqdist(qx, qy, a.sx[j], a.sy[j], g.Lx, g.Ly));
+                            const double d2 = sqdist(qx, qy, a.sx[j], a.sy[j], g.Lx, g.Ly);
+                            ok = d2 < bound2;
+                            dk = (unsigned long long)__double_as_longlong(d2);
                             ik = a.sidx[j];
                         }
                         const unsigned bal = __ballot_sync(0xffffffffu, ok);
@@ -379,18 +387,43 @@ __global__ void __launch_bounds__(kWarps * 32) query_kernel(QueryArgs a) {
                 R += max(1, R / 2);
                 continue;
             }
-            // rank the buffer, write the k best
+            // rank the buffer, write the k best: one pass over the buffer, each
+            // (broadcast) entry compared with all of the lane's own entries
             int myrank[kCap / 32];
+            unsigned long long mine_d[kCap / 32];
+            int mine_i[kCap / 32];
+            const int nslot = (have + 31) / 32;  // warp-uniform
 #pragma unroll
             for (int u = 0; u < kCap / 32; ++u) {
                 const int c = lane + 32 * u;
-                int rank = kCap;
-                if (c < have) {
-                    rank = 0;
-                    for (int v = 0; v < have; ++v) rank += key_less(d[v], id[v], d[c], id[c]);
-                }
-                myrank[u] = rank;
+                myrank[u] = 0;
+                mine_d[u] = (u < nslot && c < have) ? d[c] : 0ull;
+                mine_i[u] = (u < nslot && c < have) ? id[c] : 0;
             }
+            // the slot count is warp-uniform: one loop body per count, so only
+            // the live slots are compared
+            auto rank_with = [&](auto ns) {
+                constexpr int NS = decltype(ns)::value;
+                for (int v = 0; v < have; ++v) {
+                    const unsigned long long dv = d[v];
+                    const int iv = id[v];
+#pragma unroll
+                    for (int u = 0; u < NS; ++u) myrank[u] += key_less(dv, iv, mine_d[u], mine_i[u]);
+                }
+            };
+            switch (nslot) {
+                case 1: rank_with(std::integral_constant<int, 1>{}); break;
+                case 2: rank_with(std::integral_constant<int, 2>{}); break;
+                case 3: rank_with(std::integral_constant<int, 3>{}); break;
+                case 4: rank_with(std::integral_constant<int, 4>{}); break;
+                case 5: rank_with(std::integral_constant<int, 5>{}); break;
+                case 6: rank_with(std::integral_constant<int, 6>{}); break;
+                case 7: rank_with(std::integral_constant<int, 7>{}); break;
+                default: rank_with(std::integral_constant<int, kCap / 32>{}); break;
+            }
+#pragma unroll
+            for (int u = 0; u < kCap / 32; ++u)
+                if (lane + 32 * u >= have) myrank[u] = kCap;
             // k-th distance: the entry of rank k-1, broadcast by two max-reductions
             unsigned long long dkth = 0;
 #pragma unroll
