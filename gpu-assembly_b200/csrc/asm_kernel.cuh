@@ -220,120 +220,182 @@ __device__ __forceinline__ double rhs_poly(const AsmParams& p, int q, int m, int
 }
 
 // Gaussian elimination with row-implicit partial pivoting on the matrix in
-// shared memory (systems too large for register rows). Lane (lr, lc) owns
-// rows lr + GR*sl and columns c = lc (mod GC). Per step: pivot search on the
-// lanes' rows (the same packed keys and reductions as the register path),
-// multipliers l = a(r,c) * (1/pivot) kept in place as the L factor, and the
-// update a(r,j) -= l * a(p,j) of the lane's rows over its columns j > c; the
-// right-hand sides (X, shared) likewise. On return yv holds the transformed
-// right-hand sides of the lane's rows, pst/dinv/pivrow as the register path.
+// shared memory (systems too large for register rows), blocked right-looking.
+// Lane (lr, lc) owns rows lr + GR*sl and columns c = lc (mod GC). The
+// columns go in panels of PB:
+//   A. the panel's PB steps, each: pivot search on the lanes' rows (the same
+//      packed keys and reductions as the register path), multipliers
+//      l = a(r,c) * (1/pivot) kept in place as the L factor, the update
+//      a(r,j) -= l * a(p,j) confined to the panel's columns, and the
+//      right-hand sides (X, shared);
+//   B. the panel's pivot rows over the trailing columns: row p_t receives
+//      the updates of steps t' < t, in order (a triangular pass spread over
+//      all lanes by column);
+//   C. every row not yet pivoted, over the trailing columns: the PB updates
+//      of the panel, in order, with one load and one store per element.
+// Each element sees exactly the fused multiply-adds of the unblocked
+// elimination, in the same order, so the result is bit-identical to it; the
+// shared-memory traffic of the trailing update drops by PB.
+// On return yv holds the transformed right-hand sides of the lane's rows,
+// pst/dinv/pivrow as the register path.
 template <typename T, int GR, int GC, int NTP, int NRHS, typename C>
 __device__ __forceinline__ void eliminate_smem(T* S, T* X, T* buf, int* pivrow, T (&yv)[C::R][NRHS],
                                                int (&pst)[C::R], T (&dinv)[C::R], int& info,
                                                int lr, int lc, int lg, unsigned gmask) {
     constexpr int R = C::R, LDS = C::LDS, G = C::G, BW = C::BW;
+    constexpr int PB = 8;  // panel width
+    static_assert(NTP % PB == 0, "whole panels");
 #pragma unroll
     for (int sl = 0; sl < R; ++sl) {
         pst[sl] = kFree;
         dinv[sl] = T(0);
     }
 #pragma unroll 1
-    for (int c = 0; c < NTP; ++c) {
-        const int sc = C::scol(c);
-        // pivot search over the lanes' rows (lane-column 0 only)
-        int prow;
-        bool zero_pivot;
-        T my_inv, lbest = T(1);
-        if constexpr (sizeof(T) == 4) {
-            uint32_t best = 0;
-#pragma unroll
-            for (int sl = 0; sl < R; ++sl) {
-                const int r = lr + GR * sl;
-                const T v = S[r * LDS + sc];
-                const uint32_t kk = (lc == 0 && pst[sl] == kFree)
-                                        ? ((((__float_as_uint(fabsf(v)) >> 7) + 1u) << 7) |
-                                           (uint32_t)(127 - r))
-                                        : 0u;
-                if (kk > best) {
-                    best = kk;
-                    lbest = v;
-                }
-            }
-            my_inv = __frcp_rn(lbest);
-            const uint32_t m = __reduce_max_sync(gmask, best);
-            prow = 127 - (int)(m & 127u);
-            zero_pivot = (m >> 7) <= 1u;
-        } else {
-            uint32_t bhi = 0, blo = 0;
-#pragma unroll
-            for (int sl = 0; sl < R; ++sl) {
-                const int r = lr + GR * sl;
-                const T v = S[r * LDS + sc];
-                const unsigned long long bits =
-                    (unsigned long long)__double_as_longlong(fabs((double)v));
-                const bool ok = lc == 0 && pst[sl] == kFree;
-                const uint32_t hi = ok ? (uint32_t)(bits >> 32) + 1u : 0u;
-                const uint32_t lo =
-                    ok ? ((((uint32_t)bits) >> 7) << 7) | (uint32_t)(127 - r) : 0u;
-                if (hi > bhi || (hi == bhi && lo > blo)) {
-                    bhi = hi;
-                    blo = lo;
-                    lbest = v;
-                }
-            }
-            my_inv = __drcp_rn(lbest);
-            const uint32_t mh = __reduce_max_sync(gmask, bhi);
-            const uint32_t ml = __reduce_max_sync(gmask, bhi == mh ? blo : 0u);
-            prow = 127 - (int)(ml & 127u);
-            zero_pivot = mh <= 1u && (ml >> 7) == 0u;
-        }
-        if (zero_pivot && info == 0) info = c + 1;
-        const int plr = prow % GR, psl = prow / GR;
-        if (lg == 0) pivrow[c] = prow;
-        // the owner publishes 1/pivot; everybody marks the pivot row used
-        if (lr == plr && lc == 0) buf[BW - 1] = my_inv;
-        __syncwarp(gmask);
-        const T inv = buf[BW - 1];
-#pragma unroll
-        for (int sl = 0; sl < R; ++sl)
-            if (lr == plr && sl == psl) {
-                pst[sl] = c;
-                dinv[sl] = inv;
-            }
-        // multipliers of the lane's unused rows
-        T l[R];
-#pragma unroll
-        for (int sl = 0; sl < R; ++sl) {
-            const int r = lr + GR * sl;
-            l[sl] = (pst[sl] == kFree) ? S[r * LDS + sc] * inv : T(0);
-        }
-        __syncwarp(gmask);  // everybody has read column c
-        if (lc == 0) {
-#pragma unroll
-            for (int sl = 0; sl < R; ++sl)
-                if (pst[sl] == kFree) S[(lr + GR * sl) * LDS + sc] = l[sl];
-        }
-        // update: the lane's rows over its columns j > c, then the right-hand sides
-        const T* Sp = S + prow * LDS;
-        for (int j = c + 1 + ((lc - c - 1) % GC + GC) % GC; j < NTP; j += GC) {
-            const int sj = C::scol(j);
-            const T u = Sp[sj];
-#pragma unroll
-            for (int sl = 0; sl < R; ++sl) {
-                if (pst[sl] != kFree) continue;  // rows already pivoted stay as they are
-                T* e = S + (lr + GR * sl) * LDS + sj;
-                *e = fma(-l[sl], u, *e);
-            }
-        }
-        if (lc == 0) {
-#pragma unroll
-            for (int q = 0; q < NRHS; ++q) {
-                const T u = X[prow * NRHS + q];
+    for (int c0 = 0; c0 < NTP; c0 += PB) {
+        // ---- A. the panel's steps
+#pragma unroll 1
+        for (int c = c0; c < c0 + PB; ++c) {
+            const int sc = C::scol(c);
+            // pivot search over the lanes' rows (lane-column 0 only)
+            int prow;
+            bool zero_pivot;
+            T my_inv, lbest = T(1);
+            if constexpr (sizeof(T) == 4) {
+                uint32_t best = 0;
 #pragma unroll
                 for (int sl = 0; sl < R; ++sl) {
-                    T* e = X + (lr + GR * sl) * NRHS + q;
-                    if (pst[sl] == kFree) *e = fma(-l[sl], u, *e);
+                    const int r = lr + GR * sl;
+                    const T v = S[r * LDS + sc];
+                    const uint32_t kk = (lc == 0 && pst[sl] == kFree)
+                                            ? ((((__float_as_uint(fabsf(v)) >> 7) + 1u) << 7) |
+                                               (uint32_t)(127 - r))
+                                            : 0u;
+                    if (kk > best) {
+                        best = kk;
+                        lbest = v;
+                    }
                 }
+                my_inv = __frcp_rn(lbest);
+                const uint32_t m = __reduce_max_sync(gmask, best);
+                prow = 127 - (int)(m & 127u);
+                zero_pivot = (m >> 7) <= 1u;
+            } else {
+                uint32_t bhi = 0, blo = 0;
+#pragma unroll
+                for (int sl = 0; sl < R; ++sl) {
+                    const int r = lr + GR * sl;
+                    const T v = S[r * LDS + sc];
+                    const unsigned long long bits =
+                        (unsigned long long)__double_as_longlong(fabs((double)v));
+                    const bool ok = lc == 0 && pst[sl] == kFree;
+                    const uint32_t hi = ok ? (uint32_t)(bits >> 32) + 1u : 0u;
+                    const uint32_t lo =
+                        ok ? ((((uint32_t)bits) >> 7) << 7) | (uint32_t)(127 - r) : 0u;
+                    if (hi > bhi || (hi == bhi && lo > blo)) {
+                        bhi = hi;
+                        blo = lo;
+                        lbest = v;
+                    }
+                }
+                my_inv = __drcp_rn(lbest);
+                const uint32_t mh = __reduce_max_sync(gmask, bhi);
+                const uint32_t ml = __reduce_max_sync(gmask, bhi == mh ? blo : 0u);
+                prow = 127 - (int)(ml & 127u);
+                zero_pivot = mh <= 1u && (ml >> 7) == 0u;
+            }
+            if (zero_pivot && info == 0) info = c + 1;
+            const int plr = prow % GR, psl = prow / GR;
+            if (lg == 0) pivrow[c] = prow;
+            // the owner publishes 1/pivot; everybody marks the pivot row used
+            if (lr == plr && lc == 0) buf[BW - 1] = my_inv;
+            __syncwarp(gmask);
+            const T inv = buf[BW - 1];
+#pragma unroll
+            for (int sl = 0; sl < R; ++sl)
+                if (lr == plr && sl == psl) {
+                    pst[sl] = c;
+                    dinv[sl] = inv;
+                }
+            // multipliers of the lane's unused rows
+            T l[R];
+#pragma unroll
+            for (int sl = 0; sl < R; ++sl) {
+                const int r = lr + GR * sl;
+                l[sl] = (pst[sl] == kFree) ? S[r * LDS + sc] * inv : T(0);
+            }
+            __syncwarp(gmask);  // everybody has read column c
+            if (lc == 0) {
+#pragma unroll
+                for (int sl = 0; sl < R; ++sl)
+                    if (pst[sl] == kFree) S[(lr + GR * sl) * LDS + sc] = l[sl];
+            }
+            // update: the lane's rows over its panel columns j > c, then the
+            // right-hand sides
+            const T* Sp = S + prow * LDS;
+            for (int j = c + 1 + ((lc - c - 1) % GC + GC) % GC; j < c0 + PB; j += GC) {
+                const int sj = C::scol(j);
+                const T u = Sp[sj];
+#pragma unroll
+                for (int sl = 0; sl < R; ++sl) {
+                    if (pst[sl] != kFree) continue;  // rows already pivoted stay as they are
+                    T* e = S + (lr + GR * sl) * LDS + sj;
+                    *e = fma(-l[sl], u, *e);
+                }
+            }
+            if (lc == 0) {
+#pragma unroll
+                for (int q = 0; q < NRHS; ++q) {
+                    const T u = X[prow * NRHS + q];
+#pragma unroll
+                    for (int sl = 0; sl < R; ++sl) {
+                        T* e = X + (lr + GR * sl) * NRHS + q;
+                        if (pst[sl] == kFree) *e = fma(-l[sl], u, *e);
+                    }
+                }
+            }
+            __syncwarp(gmask);
+        }
+        const int jt = c0 + PB;  // first trailing column
+        if (jt >= NTP) break;
+        int prw[PB];  // the panel's pivot rows
+#pragma unroll
+        for (int t = 0; t < PB; ++t) prw[t] = pivrow[c0 + t];
+        // ---- B. the panel's pivot rows over the trailing columns
+        for (int j = jt + lg; j < NTP; j += G) {
+            const int sj = C::scol(j);
+            T u[PB];
+#pragma unroll
+            for (int t = 0; t < PB; ++t) {
+                T* e = S + prw[t] * LDS + sj;
+                T v = *e;
+#pragma unroll
+                for (int tp = 0; tp < t; ++tp)
+                    v = fma(-S[prw[t] * LDS + C::scol(c0 + tp)], u[tp], v);
+                *e = v;
+                u[t] = v;
+            }
+        }
+        __syncwarp(gmask);
+        // ---- C. the rows not yet pivoted over the trailing columns
+        T lm[R][PB];
+#pragma unroll
+        for (int sl = 0; sl < R; ++sl)
+#pragma unroll
+            for (int t = 0; t < PB; ++t)
+                lm[sl][t] = (pst[sl] == kFree) ? S[(lr + GR * sl) * LDS + C::scol(c0 + t)] : T(0);
+        for (int j = jt + ((lc - jt) % GC + GC) % GC; j < NTP; j += GC) {
+            const int sj = C::scol(j);
+            T u[PB];
+#pragma unroll
+            for (int t = 0; t < PB; ++t) u[t] = S[prw[t] * LDS + sj];
+#pragma unroll
+            for (int sl = 0; sl < R; ++sl) {
+                if (pst[sl] != kFree) continue;
+                T* e = S + (lr + GR * sl) * LDS + sj;
+                T v = *e;
+#pragma unroll
+                for (int t = 0; t < PB; ++t) v = fma(-lm[sl][t], u[t], v);
+                *e = v;
             }
         }
         __syncwarp(gmask);
