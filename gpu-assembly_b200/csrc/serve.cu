@@ -20,6 +20,7 @@
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
+#include <cstdint>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -42,8 +43,9 @@ struct Req {
     long long ticket = 0;
     int n = 0, k = 0, nrhs = 0;
     rbfb_desc desc{};
-    double* xh = nullptr;  // pinned host copies of the nodes
+    double* xh = nullptr;  // pinned host copies of the nodes (from the server's cache)
     double* yh = nullptr;
+    size_t xh_cap = 0, yh_cap = 0;
     State state = State::Queued;
     int status = RBFB_OK;
     size_t bytes = 0;
@@ -86,6 +88,14 @@ struct rbfb_server {
     std::deque<long long> queue;
     Clock::time_point t0 = Clock::now();
     cudaStream_t io = nullptr;  // fetch copies
+    // Pinned staging buffers for submitted node sets, reused: page-locking
+    // and unlocking host memory per request costs milliseconds (and
+    // unlocking may wait for the device). Blocks are never returned to the
+    // system before destroy. Own mutex, taken by the completion callback;
+    // like the server mutex it is never held across a CUDA call.
+    std::mutex pin_mu;
+    std::multimap<size_t, void*> pin_free;  // capacity -> block
+    std::vector<void*> pin_all;
     double now_ms() const {
         return std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
     }
@@ -99,6 +109,38 @@ size_t request_bytes(int n, int k, int nrhs) {
            sizeof(rbfb::DevCounters) + 1024;
 }
 
+// A pinned block of at least `bytes` (capacity in *cap), or nullptr. The
+// cache mutex is never held across the CUDA call: a completion callback
+// (pin_release) may run meanwhile, and the CUDA call may wait for it.
+void* pin_acquire(rbfb_server* s, size_t bytes, size_t* cap) {
+    {
+        std::lock_guard<std::mutex> l(s->pin_mu);
+        auto it = s->pin_free.lower_bound(bytes);
+        if (it != s->pin_free.end() && it->first <= 4 * bytes + (1u << 20)) {
+            void* p = it->second;
+            *cap = it->first;
+            s->pin_free.erase(it);
+            return p;
+        }
+    }
+    size_t c = 1u << 16;
+    while (c < bytes) c <<= 1;
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, c, cudaHostAllocDefault) != cudaSuccess) return nullptr;
+    {
+        std::lock_guard<std::mutex> l(s->pin_mu);
+        s->pin_all.push_back(p);
+    }
+    *cap = c;
+    return p;
+}
+// Back to the cache (no CUDA call: allowed in a stream callback).
+void pin_release(rbfb_server* s, void* p, size_t cap) {
+    if (!p) return;
+    std::lock_guard<std::mutex> l(s->pin_mu);
+    s->pin_free.emplace(cap, p);
+}
+
 struct CallbackArg {
     rbfb_server* srv;
     Req* req;
@@ -106,6 +148,10 @@ struct CallbackArg {
 
 void CUDART_CB on_done(void* p) {
     auto* a = static_cast<CallbackArg*>(p);
+    // the node copies ran before the kernels on this stream: staging is free
+    pin_release(a->srv, a->req->xh, a->req->xh_cap);
+    pin_release(a->srv, a->req->yh, a->req->yh_cap);
+    a->req->xh = a->req->yh = nullptr;
     {
         std::lock_guard<std::mutex> l(a->srv->mu);
         a->req->t_end = a->srv->now_ms();
@@ -205,15 +251,16 @@ void worker_loop(rbfb_server* s) {
     }
 }
 
-void free_request(Req* r) {
+void free_request(rbfb_server* s, Req* r) {
     cudaStream_t st = r->stream;
     auto fr = [&](void* p) {
         if (p) cudaFreeAsync(p, st);
     };
     fr(r->x); fr(r->y); fr(r->ja); fr(r->info); fr(r->fb); fr(r->ctr);
     for (auto& v : r->vals) fr(v);
-    if (r->xh) cudaFreeHost(r->xh);
-    if (r->yh) cudaFreeHost(r->yh);
+    // staging of a request that never completed (failed or never launched)
+    pin_release(s, r->xh, r->xh_cap);
+    pin_release(s, r->yh, r->yh_cap);
     r->xh = r->yh = nullptr;
 }
 
@@ -241,6 +288,15 @@ int rbfb_server_create(rbfb_server** out, int device, size_t budget, int max_slo
         }
     }
     cudaStreamCreateWithFlags(&s->io, cudaStreamNonBlocking);
+    // Requests allocate from the device's default stream-ordered pool; let it
+    // keep up to the budget cached between requests instead of handing memory
+    // back to the driver at every synchronisation (an attribute of this
+    // process's pool, not a setting of the GPU).
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = budget;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     s->worker = std::thread(worker_loop, s);
     *out = s;
     return RBFB_OK;
@@ -266,9 +322,13 @@ int rbfb_server_submit(rbfb_server* s, const rbfb_request* req, long long* ticke
     r->desc = d;
     r->bytes = request_bytes(req->n, req->k, nrhs);
     if (r->bytes > s->budget) return RBFB_EBUDGET;
-    if (cudaHostAlloc(&r->xh, r->n * 8, cudaHostAllocDefault) != cudaSuccess ||
-        cudaHostAlloc(&r->yh, r->n * 8, cudaHostAllocDefault) != cudaSuccess)
+    r->xh = static_cast<double*>(pin_acquire(s, r->n * 8, &r->xh_cap));
+    r->yh = static_cast<double*>(pin_acquire(s, r->n * 8, &r->yh_cap));
+    if (!r->xh || !r->yh) {
+        pin_release(s, r->xh, r->xh_cap);
+        pin_release(s, r->yh, r->yh_cap);
         return RBFB_ENOMEM;
+    }
     std::memcpy(r->xh, req->x_h, r->n * 8);
     std::memcpy(r->yh, req->y_h, r->n * 8);
     {
@@ -362,7 +422,7 @@ int rbfb_server_release(rbfb_server* s, long long ticket) {
         s->resident -= std::min(s->resident, r->bytes);
     }
     cudaSetDevice(s->device);
-    free_request(r.get());
+    free_request(s, r.get());
     s->cv.notify_all();
     return RBFB_OK;
 }
@@ -384,13 +444,14 @@ int rbfb_server_destroy(rbfb_server* s) {
     if (s->worker.joinable()) s->worker.join();
     cudaSetDevice(s->device);
     for (auto& sl : s->slots) cudaStreamSynchronize(sl.stream);
-    for (auto& kv : s->reqs) free_request(kv.second.get());
+    for (auto& kv : s->reqs) free_request(s, kv.second.get());
     for (auto& sl : s->slots) {
         cudaStreamSynchronize(sl.stream);
         cudaStreamDestroy(sl.stream);
         rbfb_destroy(sl.ctx);
     }
     if (s->io) cudaStreamDestroy(s->io);
+    for (void* p : s->pin_all) cudaFreeHost(p);
     delete s;
     return RBFB_OK;
 }
