@@ -175,3 +175,21 @@ def test_csr_batch_graph_replay(ctx, torch_cuda):
     np.testing.assert_array_equal(outs[0], outs[2])
     Wo, _ = O.assemble_csr(x, y, ia, ja, degree=deg, P=2, Q=0)
     np.testing.assert_array_equal(outs[0], Wo)  # FP64 path: bit-identical to the oracle
+
+
+@pytest.mark.parametrize("workload", ["disk", "bump"])
+def test_workload_runner_small(torch_cuda, capsys, workload):
+    # the benchmark workloads at a small size: every stencil solved, the mixed
+    # form within its bound of the FP64 form (degree 4 at cond ~1e6..1e7: the
+    # mixed form's FP64 fallback keeps it within 1e-9)
+    import json
+    from rbf_b200 import run
+    run.main(["--workload", workload, "--n", "20000", "--precision", "both", "--reps", "1"])
+    out = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert out["stencils"] == 20000
+    for form in ("fp64", "mixed"):
+        assert out[form]["bad_info"] == 0
+        assert out[form]["stats"]["stencils"] == 20000
+    assert out["mixed_max_rel_err_vs_fp64"] <= 1e-9
+    if workload == "disk":
+        assert out["fp64"]["stats"]["buckets"] >= 3
