@@ -330,28 +330,41 @@ __device__ __forceinline__ void eliminate_smem(T* S, T* X, T* buf, int* pivrow, 
                     if (pst[sl] == kFree) S[(lr + GR * sl) * LDS + sc] = l[sl];
             }
             // update: the lane's rows over its panel columns j > c, then the
-            // right-hand sides
+            // right-hand sides. All rows are loaded and updated branch-free
+            // (independent chains the compiler can interleave); only the rows
+            // not yet pivoted are stored back, so pivoted rows stay as they are.
             const T* Sp = S + prow * LDS;
             for (int j = c + 1 + ((lc - c - 1) % GC + GC) % GC; j < c0 + PB; j += GC) {
                 const int sj = C::scol(j);
                 const T u = Sp[sj];
+                T v[R];
 #pragma unroll
-                for (int sl = 0; sl < R; ++sl) {
-                    if (pst[sl] != kFree) continue;  // rows already pivoted stay as they are
-                    T* e = S + (lr + GR * sl) * LDS + sj;
-                    *e = fma(-l[sl], u, *e);
-                }
+                for (int sl = 0; sl < R; ++sl) v[sl] = S[(lr + GR * sl) * LDS + sj];
+#pragma unroll
+                for (int sl = 0; sl < R; ++sl) v[sl] = fma(-l[sl], u, v[sl]);
+#pragma unroll
+                for (int sl = 0; sl < R; ++sl)
+                    if (pst[sl] == kFree) S[(lr + GR * sl) * LDS + sj] = v[sl];
             }
             if (lc == 0) {
+                T uq[NRHS];
 #pragma unroll
-                for (int q = 0; q < NRHS; ++q) {
-                    const T u = X[prow * NRHS + q];
+                for (int q = 0; q < NRHS; ++q) uq[q] = X[prow * NRHS + q];
+                T v[R][NRHS];
 #pragma unroll
-                    for (int sl = 0; sl < R; ++sl) {
-                        T* e = X + (lr + GR * sl) * NRHS + q;
-                        if (pst[sl] == kFree) *e = fma(-l[sl], u, *e);
+                for (int sl = 0; sl < R; ++sl)
+#pragma unroll
+                    for (int q = 0; q < NRHS; ++q) v[sl][q] = X[(lr + GR * sl) * NRHS + q];
+#pragma unroll
+                for (int sl = 0; sl < R; ++sl)
+#pragma unroll
+                    for (int q = 0; q < NRHS; ++q) v[sl][q] = fma(-l[sl], uq[q], v[sl][q]);
+#pragma unroll
+                for (int sl = 0; sl < R; ++sl)
+                    if (pst[sl] == kFree) {
+#pragma unroll
+                        for (int q = 0; q < NRHS; ++q) X[(lr + GR * sl) * NRHS + q] = v[sl][q];
                     }
-                }
             }
             __syncwarp(gmask);
         }
@@ -388,15 +401,18 @@ __device__ __forceinline__ void eliminate_smem(T* S, T* X, T* buf, int* pivrow, 
             T u[PB];
 #pragma unroll
             for (int t = 0; t < PB; ++t) u[t] = S[prw[t] * LDS + sj];
+            // R independent chains, interleaved step by step; each element
+            // still takes the PB updates in order t = 0..PB-1
+            T v[R];
 #pragma unroll
-            for (int sl = 0; sl < R; ++sl) {
-                if (pst[sl] != kFree) continue;
-                T* e = S + (lr + GR * sl) * LDS + sj;
-                T v = *e;
+            for (int sl = 0; sl < R; ++sl) v[sl] = S[(lr + GR * sl) * LDS + sj];
 #pragma unroll
-                for (int t = 0; t < PB; ++t) v = fma(-lm[sl][t], u[t], v);
-                *e = v;
-            }
+            for (int t = 0; t < PB; ++t)
+#pragma unroll
+                for (int sl = 0; sl < R; ++sl) v[sl] = fma(-lm[sl][t], u[t], v[sl]);
+#pragma unroll
+            for (int sl = 0; sl < R; ++sl)
+                if (pst[sl] == kFree) S[(lr + GR * sl) * LDS + sj] = v[sl];
         }
         __syncwarp(gmask);
     }
