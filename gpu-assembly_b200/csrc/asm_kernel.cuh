@@ -18,29 +18,34 @@
 // which the row in slot s became the pivot row (kFree while unused).
 //
 // Phases of one stencil:
-//   gather   lanes load ja and the neighbour coordinates (FP64), shift to the
-//            centre (minimum image in a periodic box) and take the group max
-//            of the binary exponents for the power-of-two radius scale;
+//   gather   lanes take ja and the neighbour coordinates (FP64) -- from
+//            shared memory when the previous stencil's call prefetched them
+//            with cp.async (PF shapes), else from global memory -- shift to
+//            the centre (minimum image in a periodic box) and take the group
+//            max of the binary exponents for the power-of-two radius scale;
 //   fill     phi for each unordered node pair once, monomials per node, the
 //            right-hand sides per row: all FP64, written (rounded to T) into
-//            a shared-memory staging matrix S, then vector-loaded into the
-//            row registers;
-//   factor   per step c (fully unrolled, all register indices static):
-//            redux.max over the group on the |a(r,c)| bit patterns of unused
-//            rows, redux.min on the row index among the maxima (ties go to
-//            the lowest row, as in the oracle); the pivot row's owner lanes
-//            write it to a double-buffered shared row, __syncwarp, every lane
-//            reads it back (broadcast); l = a(r,c) * (1/pivot) for unused rows
+//            a shared-memory staging matrix S, then loaded into the row
+//            registers (register shapes);
+//   factor   register shapes: a runtime loop over blocks of GC*VEC steps,
+//            the steps of a block unrolled (register indices static). Per
+//            step: the pivot found by the look-ahead reduction (packed keys:
+//            |a(r,c)| without its 7 lowest bits, the row index in those bits,
+//            ties to the lowest row as in the oracle); the pivot row's owner
+//            lanes write it to a double-buffered shared row, __syncwarp,
+//            every lane reads it back; l = a(r,c) * (1/pivot) for unused rows
 //            (0 otherwise); a(r,j) = fma(-l, u(j), a(r,j)) for j > c and for
-//            the right-hand sides; l is kept in a(r,c) (the L factor);
-//   solve    the factors go back to S, the registers die; column-oriented
-//            back substitution from S: x_c = y(p_c) * (1/pivot_c), then
-//            y(r) = fma(-u(r,c), x_c, y(r)) for rows pivoted before c;
+//            the right-hand sides; l is kept in a(r,c) (the L factor).
+//            Shared-memory shapes (n up to 80): the same steps on S, blocked
+//            right-looking in panels (eliminate_smem);
+//   solve    the factors are in S; column-oriented back substitution from S:
+//            x_c = y(p_c) * (1/pivot_c), then y(r) = fma(-u(r,c), x_c, y(r))
+//            for rows pivoted before c;
 //   refine   (MIXED: factor in FP32) residual b - M x in FP64 from the FP64
 //            phi cache and monomials in shared memory, correction through
-//            the FP32 factors in S, x += d in FP64, until
-//            max|d| <= tol * max|x| per right-hand side; a stencil that
-//            stalls or runs out of sweeps is queued for the FP64 kernel;
+//            the FP32 factors in S, x += d in FP64, until the predicted
+//            remaining error is below the tolerance; a stencil that stalls,
+//            diverges or runs out of sweeps is queued for the FP64 kernel;
 //   scatter  weights of the k node unknowns, rescaled by 2^(-order*e), to
 //            values[q][row offset + j] (coalesced over j).
 #pragma once
