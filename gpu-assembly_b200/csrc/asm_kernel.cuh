@@ -125,7 +125,7 @@ struct AsmCfg {
     static constexpr int KMAX = NTP - NP;
     static constexpr int NPAIR = KMAX * (KMAX - 1) / 2;  // packed strict upper triangle
     static constexpr int KPL = (KMAX + G - 1) / G;       // gathered nodes per lane
-    static constexpr int VEC = 16 / sizeof(T);
+    static constexpr int VEC = 2;  // register tuples: float2 / double2
     static_assert(SMEM || CW % VEC == 0, "register columns must tile the vector width");
     static_assert(NTP <= 128, "pivot keys carry the row index in 7 bits");
     // pivot row buffer: NTP columns, NRHS right-hand sides, the pivot's reciprocal
@@ -134,7 +134,7 @@ struct AsmCfg {
     // substitution, the refinement sweeps, the shared-memory elimination) and
     // write it across rows (the fill), so consecutive rows must start in
     // different banks: an odd stride in elements for the shared-memory
-    // elimination; for the register path, whose rows move as 16-byte tuples,
+    // elimination; for the register path, whose rows move as tuples,
     // an odd stride in tuples (at most two rows of a column share a bank).
     static constexpr int LDS = SMEM ? NTP + 1 : ((NTP / VEC) % 2 == 0 ? NTP + VEC : NTP);
     static constexpr int al16(int b) { return (b + 15) & ~15; }
@@ -158,21 +158,22 @@ struct AsmCfg {
     static __device__ __forceinline__ int scol(int c) { return (c % GC) * CW + c / GC; }
 };
 
-// Register rows are kept as 16-byte tuples (float4 / double2) so the pivot
-// row goes to shared memory straight from aligned register quads.
+// Register rows are kept as two-element tuples (float2 / double2) so the
+// pivot row goes to shared memory straight from aligned register pairs. A
+// block of the elimination covers GC * 2 steps; for FP32, wider float4
+// tuples would double the unrolled steps per block (and the code size)
+// for no fewer shared-memory instructions that matter.
 template <typename T>
 struct Vec;
 template <>
 struct Vec<float> {
-    using type = float4;
+    using type = float2;
 };
 template <>
 struct Vec<double> {
     using type = double2;
 };
-__device__ __forceinline__ float& comp(float4& v, int t) {
-    return t == 0 ? v.x : (t == 1 ? v.y : (t == 2 ? v.z : v.w));
-}
+__device__ __forceinline__ float& comp(float2& v, int t) { return t == 0 ? v.x : v.y; }
 __device__ __forceinline__ double& comp(double2& v, int t) { return t == 0 ? v.x : v.y; }
 
 // Packed index of the pair (i, j), i < j, of a k-node stencil.

@@ -17,7 +17,7 @@ RBFB_VARIANT(f64_p2q3_n32_g16x1, double, 16, 1, 32, 3, 2, 3, false, 64, 1, false
 RBFB_VARIANT(f64_p3q5_n48_g16x2, double, 16, 2, 48, 3, 3, 5, false, 64, 1, false, false)
 RBFB_VARIANT(mix_p2q3_n32_g16x1, float, 16, 1, 32, 3, 2, 3, true, 64, 1, false, true)
 RBFB_VARIANT(mix_p2q3_n32_g16x2, float, 16, 2, 32, 3, 2, 3, true, 64, 1, false, true)
-RBFB_VARIANT(mix_p3q5_n48_g16x2, float, 16, 2, 48, 3, 3, 5, true, 64, 6, false, true)
+RBFB_VARIANT(mix_p3q5_n48_g16x2, float, 16, 2, 48, 3, 3, 5, true, 64, 4, false, true)
 RBFB_VARIANT(mix_p3q5_n48_g16x1, float, 16, 1, 48, 3, 3, 5, true, 64, 1, false, true)
 RBFB_VARIANT(f64_p4q7_n64_smem, double, 16, 2, 64, 3, 4, 7, false, 32, 1, true, true)
 RBFB_VARIANT(f64_p4q7_n80_smem, double, 16, 2, 80, 3, 4, 7, false, 32, 1, true, true)
