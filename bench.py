@@ -362,8 +362,8 @@ def main():
     e2e_ms = max_over_ranks(1e3 * (t1 - t0) / e2e_steps)
 
     # ---- serving sample (rank 0 only)
-    serving = None
-    if rank == 0 and not args.no_serve and args.serve_requests > 0:
+    serving = None  # a one-GPU measurement: taken at N = 1 only
+    if ws == 1 and not args.no_serve and args.serve_requests > 0:
         serving = serve_sample(R, NS, local, args.serve_requests,
                                "fp64" if d_head is d_f64 else "mixed")
 
@@ -433,7 +433,7 @@ def main():
     }
     if serving is not None:
         line["serving"] = serving
-    if not args.no_cpu:
+    if ws == 1 and not args.no_cpu:  # the host-core baseline: rank 0 at N = 1 only
         line["cpu_baseline"] = cpu_baseline_sample()
     print(json.dumps(line), flush=True)
     ctx.close()
