@@ -29,9 +29,10 @@
 //            registers (register shapes);
 //   factor   register shapes: a runtime loop over blocks of GC*VEC steps,
 //            the steps of a block unrolled (register indices static). Per
-//            step: the pivot found by the look-ahead reduction (packed keys:
-//            |a(r,c)| without its 7 lowest bits, the row index in those bits,
-//            ties to the lowest row as in the oracle); the pivot row's owner
+//            step: the pivot found by the look-ahead reduction (one 32-bit
+//            key per candidate, pivot_key: the magnitude word without its 7
+//            lowest bits, the row index in those bits, ties to the lowest row
+//            as in the oracle); the pivot row's owner
 //            lanes write it to a double-buffered shared row, __syncwarp,
 //            every lane reads it back; l = a(r,c) * (1/pivot) for unused rows
 //            (0 otherwise); a(r,j) = fma(-l, u(j), a(r,j)) for j > c and for
@@ -106,6 +107,22 @@ __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
                  : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Pivot keys. The magnitude word of a candidate: the bits of |v| for
+// float, the high 32 bits of |v|'s binary64 representation (sign, exponent,
+// 20 leading mantissa bits) for double. A key is that word without its 7
+// lowest bits, plus one (an unused zero still counts), with the row index
+// (as 127 - r, so ties go to the lowest row) in the freed bits: one 32-bit
+// warp reduction finds the pivot. The oracle compares the same words.
+__device__ __forceinline__ uint32_t mag32(float v) { return __float_as_uint(fabsf(v)); }
+__device__ __forceinline__ uint32_t mag32(double v) {
+    return (uint32_t)((unsigned long long)__double_as_longlong(fabs(v)) >> 32);
+}
+__device__ __forceinline__ uint32_t pivot_key(uint32_t mag, int r) {
+    return (((mag >> 7) + 1u) << 7) | (uint32_t)(127 - r);
+}
+__device__ __forceinline__ float recip_rn(float v) { return __frcp_rn(v); }
+__device__ __forceinline__ double recip_rn(double v) { return __drcp_rn(v); }
 
 __device__ __forceinline__ unsigned group_mask(int G) {
     if (G == 32) return 0xffffffffu;
@@ -230,7 +247,7 @@ __device__ __forceinline__ double rhs_poly(const AsmParams& p, int q, int m, int
 // Lane (lr, lc) owns rows lr + GR*sl and columns c = lc (mod GC). The
 // columns go in panels of PB:
 //   A. the panel's PB steps, each: pivot search on the lanes' rows (the same
-//      packed keys and reductions as the register path), multipliers
+//      keys and reduction as the register path), multipliers
 //      l = a(r,c) * (1/pivot) kept in place as the L factor, the update
 //      a(r,j) -= l * a(p,j) confined to the panel's columns, and the
 //      right-hand sides (X, shared);
@@ -262,52 +279,27 @@ __device__ __forceinline__ void eliminate_smem(T* S, T* X, T* buf, int* pivrow, 
 #pragma unroll 1
         for (int c = c0; c < c0 + PB; ++c) {
             const int sc = C::scol(c);
-            // pivot search over the lanes' rows (lane-column 0 only)
+            // pivot search over the lanes' rows (lane-column 0 only; pivot_key)
             int prow;
             bool zero_pivot;
-            T my_inv, lbest = T(1);
-            if constexpr (sizeof(T) == 4) {
+            T my_inv;
+            {
+                T lbest = T(1);
                 uint32_t best = 0;
 #pragma unroll
                 for (int sl = 0; sl < R; ++sl) {
                     const int r = lr + GR * sl;
                     const T v = S[r * LDS + sc];
-                    const uint32_t kk = (lc == 0 && pst[sl] == kFree)
-                                            ? ((((__float_as_uint(fabsf(v)) >> 7) + 1u) << 7) |
-                                               (uint32_t)(127 - r))
-                                            : 0u;
+                    const uint32_t kk = (lc == 0 && pst[sl] == kFree) ? pivot_key(mag32(v), r) : 0u;
                     if (kk > best) {
                         best = kk;
                         lbest = v;
                     }
                 }
-                my_inv = __frcp_rn(lbest);
+                my_inv = recip_rn(lbest);
                 const uint32_t m = __reduce_max_sync(gmask, best);
                 prow = 127 - (int)(m & 127u);
                 zero_pivot = (m >> 7) <= 1u;
-            } else {
-                uint32_t bhi = 0, blo = 0;
-#pragma unroll
-                for (int sl = 0; sl < R; ++sl) {
-                    const int r = lr + GR * sl;
-                    const T v = S[r * LDS + sc];
-                    const unsigned long long bits =
-                        (unsigned long long)__double_as_longlong(fabs((double)v));
-                    const bool ok = lc == 0 && pst[sl] == kFree;
-                    const uint32_t hi = ok ? (uint32_t)(bits >> 32) + 1u : 0u;
-                    const uint32_t lo =
-                        ok ? ((((uint32_t)bits) >> 7) << 7) | (uint32_t)(127 - r) : 0u;
-                    if (hi > bhi || (hi == bhi && lo > blo)) {
-                        bhi = hi;
-                        blo = lo;
-                        lbest = v;
-                    }
-                }
-                my_inv = __drcp_rn(lbest);
-                const uint32_t mh = __reduce_max_sync(gmask, bhi);
-                const uint32_t ml = __reduce_max_sync(gmask, bhi == mh ? blo : 0u);
-                prow = 127 - (int)(ml & 127u);
-                zero_pivot = mh <= 1u && (ml >> 7) == 0u;
             }
             if (zero_pivot && info == 0) info = c + 1;
             const int plr = prow % GR, psl = prow / GR;
@@ -688,57 +680,27 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, int sn, 
     // Pivot search with look-ahead: the keys of step c+1's column are formed
     // and their reduction issued as soon as that column is updated (first),
     // so the reduction runs while the rest of step c's update issues. The
-    // pivot is the unused row of largest |a(r, c)| compared without the 7
-    // lowest bits of its binary representation, ties to the lowest row (the
-    // oracle's rule); the row index rides in those 7 bits. Used rows send 0.
-    uint32_t pm_hi = 0, pm_lo = 0;  // reduced key of the next pivot (FP32: pm_hi only)
-    uint32_t pb_hi = 0, pb_lo = 0;  // this lane's best key (FP64 second phase)
-    T p_inv = T(1);                 // reciprocal of this lane's best candidate
+    // pivot is the unused row of largest key (pivot_key: the oracle's rule);
+    // used rows send 0.
+    uint32_t pm_key = 0;  // reduced key of the next pivot
+    T p_inv = T(1);       // reciprocal of this lane's best candidate
     auto keys_begin = [&](int tp, int cp, int lcc) {
         T lbest = T(1);
-        if constexpr (sizeof(T) == 4) {
-            uint32_t best = 0;
+        uint32_t best = 0;
 #pragma unroll
-            for (int sl = 0; sl < R; ++sl) {
-                const uint32_t kk =
-                    (lc == lcc && pst[sl] == kFree)
-                        ? ((((__float_as_uint(fabsf(comp(a[sl][tp], cp))) >> 7) + 1u) << 7) |
-                           (uint32_t)(127 - (lr + GR * sl)))
-                        : 0u;
-                if (kk > best) {
-                    best = kk;
-                    lbest = comp(a[sl][tp], cp);
-                }
+        for (int sl = 0; sl < R; ++sl) {
+            const T v = comp(a[sl][tp], cp);
+            const uint32_t kk =
+                (lc == lcc && pst[sl] == kFree) ? pivot_key(mag32(v), lr + GR * sl) : 0u;
+            if (kk > best) {
+                best = kk;
+                lbest = v;
             }
-            pm_hi = __reduce_max_sync(gmask, best);
-            p_inv = __frcp_rn(lbest);
-        } else {
-            uint32_t bhi = 0, blo = 0;
-#pragma unroll
-            for (int sl = 0; sl < R; ++sl) {
-                const unsigned long long bits =
-                    (unsigned long long)__double_as_longlong(fabs((double)comp(a[sl][tp], cp)));
-                const bool ok = lc == lcc && pst[sl] == kFree;
-                const uint32_t hi = ok ? (uint32_t)(bits >> 32) + 1u : 0u;
-                const uint32_t lo =
-                    ok ? ((((uint32_t)bits) >> 7) << 7) | (uint32_t)(127 - (lr + GR * sl)) : 0u;
-                if (hi > bhi || (hi == bhi && lo > blo)) {
-                    bhi = hi;
-                    blo = lo;
-                    lbest = comp(a[sl][tp], cp);
-                }
-            }
-            pb_hi = bhi;
-            pb_lo = blo;
-            pm_hi = __reduce_max_sync(gmask, bhi);
-            p_inv = __drcp_rn(lbest);  // = the oracle's 1.0 / pivot (both rounded once)
         }
-    };
-    auto keys_finish = [&]() {
-        if constexpr (sizeof(T) == 8) pm_lo = __reduce_max_sync(gmask, pb_hi == pm_hi ? pb_lo : 0u);
+        pm_key = __reduce_max_sync(gmask, best);
+        p_inv = recip_rn(lbest);  // = the oracle's 1 / pivot (both rounded once)
     };
     keys_begin(0, 0, 0);
-    keys_finish();
     auto step_block = [&](auto width, int b) {
         constexpr int W = decltype(width)::value;
 #pragma unroll
@@ -749,13 +711,8 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, int sn, 
             // 1. the pivot found by the look-ahead
             int prow;
             bool zero_pivot;
-            if constexpr (sizeof(T) == 4) {
-                prow = 127 - (int)(pm_hi & 127u);
-                zero_pivot = (pm_hi >> 7) <= 1u;
-            } else {
-                prow = 127 - (int)(pm_lo & 127u);
-                zero_pivot = pm_hi <= 1u && (pm_lo >> 7) == 0u;
-            }
+            prow = 127 - (int)(pm_key & 127u);
+            zero_pivot = (pm_key >> 7) <= 1u;
             const T my_inv = p_inv;
             if (zero_pivot && info == 0) info = c + 1;
             const int plr = prow % GR, psl = prow / GR;
@@ -816,13 +773,8 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, int sn, 
             update_tuple(tn);
             if (tn == 1) update_tuple(0);
             if (more) keys_begin(tn, (jn % SB) / GC, jn % GC);
-            constexpr int half = 1 + (W - 1) / 2;
 #pragma unroll
-            for (int cb = 1; cb < half; ++cb)
-                if (cb != tn) update_tuple(cb);
-            if (more) keys_finish();
-#pragma unroll
-            for (int cb = half; cb < W; ++cb)
+            for (int cb = 1; cb < W; ++cb)
                 if (cb != tn) update_tuple(cb);
 #pragma unroll
             for (int q = 0; q < NRHS; ++q) {

@@ -12,7 +12,7 @@
 //            current one is solved; off where the extra live state costs the
 //            register-bound elimination more than the gather latency it hides
 // The build compiles each line as its own translation unit.
-RBFB_VARIANT(f64_p2q3_n32_g16x2, double, 16, 2, 32, 3, 2, 3, false, 64, 1, false, true)
+RBFB_VARIANT(f64_p2q3_n32_g16x2, double, 16, 2, 32, 3, 2, 3, false, 64, 6, false, true)
 RBFB_VARIANT(f64_p2q3_n32_g16x1, double, 16, 1, 32, 3, 2, 3, false, 64, 1, false, true)
 RBFB_VARIANT(f64_p3q5_n48_g16x2, double, 16, 2, 48, 3, 3, 5, false, 64, 1, false, false)
 RBFB_VARIANT(mix_p2q3_n32_g16x1, float, 16, 1, 32, 3, 2, 3, true, 64, 1, false, true)

@@ -32,8 +32,9 @@
 //     elimination with partial pivoting (Golub & Van Loan, Matrix
 //     Computations, alg. 3.4.1) in its row-implicit form: rows are never
 //     swapped; at step c the pivot is the unused row with the largest
-//     |a(r,c)| compared without the 7 lowest bits of its binary64
-//     representation, ties going to the lowest row index; multipliers are
+//     |a(r,c)| compared by the high 32 bits of its binary64 representation
+//     without their 7 lowest bits (sign, exponent and the 13 leading
+//     mantissa bits), ties going to the lowest row index; multipliers are
 //     a(r,c) * (1 / pivot); updates are fma(-l, u, a); back substitution
 //     is column oriented, x_c = y_c * (1 / pivot_c). The CUDA FP64 kernel
 //     performs the same operations in the same order.
@@ -290,8 +291,10 @@ int assemble_one(const Desc& D, int P, int Q, int s, int k, const int* idx, cons
     std::fill(used, used + n, false);
     int info = 0;
     for (int c = 0; c < n; ++c) {
-        // pivot: the unused row of largest |a(r,c)| compared without the 7
-        // lowest bits of its binary64 representation, ties to the lowest row
+        // pivot: the unused row of largest |a(r,c)| compared by the high 32
+        // bits of its binary64 representation without their 7 lowest bits
+        // (the GPU reduces this as one 32-bit key with the row index in the
+        // freed bits), ties to the lowest row
         int p = -1;
         uint64_t best = 0;
         for (int r = 0; r < n; ++r) {
@@ -299,7 +302,7 @@ int assemble_one(const Desc& D, int P, int Q, int s, int k, const int* idx, cons
             const double v = std::fabs(a[r * W + c]);
             uint64_t bits;
             std::memcpy(&bits, &v, sizeof bits);
-            const uint64_t key = (bits >> 7) + 1;  // +1: an unused zero still counts
+            const uint64_t key = ((bits >> 32) >> 7) + 1;  // +1: an unused zero still counts
             if (key > best) {
                 best = key;
                 p = r;
