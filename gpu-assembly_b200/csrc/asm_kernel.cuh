@@ -676,7 +676,11 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, int sn, 
     // are NWC, not NTP.
     constexpr int SB = GC * VEC;
     static_assert(NTP % SB == 0, "padded size must be a whole number of blocks");
-    constexpr int NWC = NV >= 4 ? 4 : NV;
+    // Width classes: more classes skip more dead tuples but compile more
+    // step bodies (instruction-cache pressure). Measured on B200: rows of 12
+    // or more tuples (n = 48; FP32 rows of 16 or 24) run fastest with 2
+    // classes, rows of 8 tuples (FP64 n = 32) with 4.
+    constexpr int NWC = NV >= 12 ? 2 : (NV >= 4 ? 4 : NV);
     // Pivot search with look-ahead: the keys of step c+1's column are formed
     // and their reduction issued as soon as that column is updated (first),
     // so the reduction runs while the rest of step c's update issues. The
