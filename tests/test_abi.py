@@ -115,3 +115,14 @@ int main() {
         return
     r = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert r.returncode == 0, r.stdout + r.stderr
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    """Without the built CUDA library the binding raises: there is no CPU
+    path to fall back on."""
+    monkeypatch.setattr(rbf_b200, "_lib", None)
+    monkeypatch.setattr(rbf_b200, "LIB_PATH", tmp_path / "missing.so")
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        rbf_b200.lib()
+    with pytest.raises(RuntimeError):
+        rbf_b200.Context(0)
