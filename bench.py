@@ -301,18 +301,21 @@ def main():
     step(d_f64)
     torch.cuda.synchronize()
     W_64 = np.stack([v.cpu().numpy()[idx] for v in vals])
-    # FP64 oracle on the sampled stencils: renumber the nodes so the sampled
-    # centres come first, then assemble just those rows
-    O.set_threads(os.cpu_count() or 1)
-    order = np.concatenate([rows, np.setdiff1d(np.arange(n), rows)])
-    inv = np.empty(n, np.int64)
-    inv[order] = np.arange(n)
-    ja_s = inv[ja_h.reshape(n, K)[rows]].astype(np.int32).ravel()
-    ia_s = (np.arange(rows.size + 1) * K).astype(np.int32)
-    Wo, _ = O.assemble_csr(x[order], y[order], ia_s, ja_s, P=P, Q=Q, period=per,
-                           nstencils=rows.size)
-    err_mix = float(O.max_rel_err(W_mix, Wo, K).max())
-    err_64 = float(O.max_rel_err(W_64, Wo, K).max())
+    # FP64 oracle on the sampled stencils (the checker; rank 0 reports it, so
+    # rank 0 alone runs it): renumber the nodes so the sampled centres come
+    # first, then assemble just those rows
+    err_mix = err_64 = None
+    if rank == 0:
+        O.set_threads(os.cpu_count() or 1)
+        order = np.concatenate([rows, np.setdiff1d(np.arange(n), rows)])
+        inv = np.empty(n, np.int64)
+        inv[order] = np.arange(n)
+        ja_s = inv[ja_h.reshape(n, K)[rows]].astype(np.int32).ravel()
+        ia_s = (np.arange(rows.size + 1) * K).astype(np.int32)
+        Wo, _ = O.assemble_csr(x[order], y[order], ia_s, ja_s, P=P, Q=Q, period=per,
+                               nstencils=rows.size)
+        err_mix = float(O.max_rel_err(W_mix, Wo, K).max())
+        err_64 = float(O.max_rel_err(W_64, Wo, K).max())
 
     # ---- timed: mixed (headline) and FP64 on the same node set
     with Clocks(local) as clk:
