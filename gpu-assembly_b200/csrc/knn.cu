@@ -301,86 +301,117 @@ __global__ void __launch_bounds__(kWarps * 32) query_kernel(QueryArgs a) {
             // farther than all of these; otherwise the block grows. (A block
             // that covers the whole domain keeps everything.)
             const double bound2 = bound >= 1e299 ? INFINITY : (bound > 0.0 ? bound * bound : 0.0);
-            // gather candidates chunk by chunk; the current best k stay at the front
+            // gather candidates chunk by chunk; the current best k stay at the front.
+            // The block is a list of runs of consecutive cells (one per row, two
+            // where a periodic row wraps). A batch of up to 32 runs is laid out
+            // flat: lane t loads run t's bounds (all loads in flight at once),
+            // a warp scan gives each run its offset, and the flat candidate
+            // list is walked 32 at a time, each lane finding its run by a
+            // shuffle binary search. The candidate set and its order are those
+            // of a row-by-row walk.
             int have = 0;  // entries in the buffer (best-so-far first)
             int total = 0;
             const int nrows = yhi - ylo + 1;
-            for (int rr = 0; rr < nrows; ++rr) {
-                int cyy = ylo + rr;
-                if (g.Ly > 0) cyy = ((cyy % g.cy) + g.cy) % g.cy;
-                // contiguous run of cells along x (up to two runs when wrapped)
-                for (int part = 0; part < 2; ++part) {
-                    int c0, c1;
-                    if (g.Lx > 0 && !fullx) {
-                        const int a0 = xlo, a1 = xhi;
-                        if (a0 < 0) {
-                            if (part == 0) { c0 = a0 + g.cx; c1 = g.cx - 1; } else { c0 = 0; c1 = a1; }
-                        } else if (a1 >= g.cx) {
-                            if (part == 0) { c0 = a0; c1 = g.cx - 1; } else { c0 = 0; c1 = a1 - g.cx; }
-                        } else {
-                            if (part == 1) break;
-                            c0 = a0; c1 = a1;
+            const int nruns = 2 * nrows;
+            for (int rb = 0; rb < nruns; rb += 32) {
+                int rbeg = 0, rlen = 0;  // this lane's run: first candidate, length
+                {
+                    const int run = rb + lane;
+                    if (run < nruns) {
+                        const int rr = run >> 1, part = run & 1;
+                        int cyy = ylo + rr;
+                        if (g.Ly > 0) cyy = ((cyy % g.cy) + g.cy) % g.cy;
+                        int c0 = 0, c1 = -1;  // empty unless set below
+                        if (g.Lx > 0 && !fullx) {
+                            const int a0 = xlo, a1 = xhi;
+                            if (a0 < 0) {
+                                if (part == 0) { c0 = a0 + g.cx; c1 = g.cx - 1; } else { c0 = 0; c1 = a1; }
+                            } else if (a1 >= g.cx) {
+                                if (part == 0) { c0 = a0; c1 = g.cx - 1; } else { c0 = 0; c1 = a1 - g.cx; }
+                            } else if (part == 0) {
+                                c0 = a0; c1 = a1;
+                            }
+                        } else if (part == 0) {
+                            c0 = xlo; c1 = xhi;
                         }
-                    } else {
-                        if (part == 1) break;
-                        c0 = xlo; c1 = xhi;
+                        if (c1 >= c0) {
+                            rbeg = a.start[cyy * g.cx + c0];
+                            rlen = a.start[cyy * g.cx + c1 + 1] - rbeg;
+                        }
                     }
-                    const int beg = a.start[cyy * g.cx + c0], end = a.start[cyy * g.cx + c1 + 1];
-                    for (int base = beg; base < end; base += 32) {
-                        const int j = base + lane;
-                        bool ok = j < end;
-                        unsigned long long dk = 0;
-                        int ik = 0;
-                        if (ok) {
-                            const double d2 = sqdist(qx, qy, a.sx[j], a.sy[j], g.Lx, g.Ly);
-                            ok = d2 < bound2;
-                            dk = (unsigned long long)__double_as_longlong(d2);
-                            ik = a.sidx[j];
-                        }
-                        const unsigned bal = __ballot_sync(0xffffffffu, ok);
-                        const int cnt = __popc(bal);
-                        if (have + cnt > kCap) {
-                            // merge: keep the k best of the buffer
-                            __syncwarp();
-                            int keepd[kCap / 32];
+                }
+                int incl = rlen;  // inclusive scan of the run lengths
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += t;
+                }
+                const int excl = incl - rlen;
+                const int btotal = __shfl_sync(0xffffffffu, incl, 31);
+                for (int base = 0; base < btotal; base += 32) {
+                    const int f = base + lane;
+                    // the run holding flat index f: the number of runs ending at or
+                    // before it (incl is non-decreasing over the lanes)
+                    int r = 0;
 #pragma unroll
-                            for (int u = 0; u < kCap / 32; ++u) {
-                                const int c = lane + 32 * u;
-                                int rank = kCap;
-                                if (c < have) {
-                                    rank = 0;
-                                    for (int v = 0; v < have; ++v)
-                                        rank += key_less(d[v], id[v], d[c], id[c]);
-                                }
-                                keepd[u] = rank;
-                            }
-                            unsigned long long td[kCap / 32];
-                            int ti[kCap / 32];
-#pragma unroll
-                            for (int u = 0; u < kCap / 32; ++u) {
-                                const int c = lane + 32 * u;
-                                td[u] = c < have ? d[c] : 0;
-                                ti[u] = c < have ? id[c] : 0;
-                            }
-                            __syncwarp();
-#pragma unroll
-                            for (int u = 0; u < kCap / 32; ++u)
-                                if (keepd[u] < k) {
-                                    d[keepd[u]] = td[u];
-                                    id[keepd[u]] = ti[u];
-                                }
-                            __syncwarp();
-                            have = min(have, k);
-                        }
-                        const int pos = have + __popc(bal & ((1u << lane) - 1u));
-                        if (ok) {
-                            d[pos] = dk;
-                            id[pos] = ik;
-                        }
-                        have += cnt;
-                        total += cnt;
+                    for (int sh = 16; sh > 0; sh >>= 1) {
+                        const int v = __shfl_sync(0xffffffffu, incl, r + sh - 1);
+                        if (v <= f) r += sh;
+                    }
+                    const int jb = __shfl_sync(0xffffffffu, rbeg, r);
+                    const int jx = __shfl_sync(0xffffffffu, excl, r);
+                    const int j = jb + (f - jx);
+                    bool ok = f < btotal;
+                    unsigned long long dk = 0;
+                    int ik = 0;
+                    if (ok) {
+                        const double d2 = sqdist(qx, qy, a.sx[j], a.sy[j], g.Lx, g.Ly);
+                        ok = d2 < bound2;
+                        dk = (unsigned long long)__double_as_longlong(d2);
+                        ik = a.sidx[j];
+                    }
+                    const unsigned bal = __ballot_sync(0xffffffffu, ok);
+                    const int cnt = __popc(bal);
+                    if (have + cnt > kCap) {
+                        // merge: keep the k best of the buffer
                         __syncwarp();
+                        int keepd[kCap / 32];
+#pragma unroll
+                        for (int u = 0; u < kCap / 32; ++u) {
+                            const int c = lane + 32 * u;
+                            int rank = kCap;
+                            if (c < have) {
+                                rank = 0;
+                                for (int v = 0; v < have; ++v)
+                                    rank += key_less(d[v], id[v], d[c], id[c]);
+                            }
+                            keepd[u] = rank;
+                        }
+                        unsigned long long td[kCap / 32];
+                        int ti[kCap / 32];
+#pragma unroll
+                        for (int u = 0; u < kCap / 32; ++u) {
+                            const int c = lane + 32 * u;
+                            td[u] = c < have ? d[c] : 0;
+                            ti[u] = c < have ? id[c] : 0;
+                        }
+                        __syncwarp();
+#pragma unroll
+                        for (int u = 0; u < kCap / 32; ++u)
+                            if (keepd[u] < k) {
+                                d[keepd[u]] = td[u];
+                                id[keepd[u]] = ti[u];
+                            }
+                        __syncwarp();
+                        have = min(have, k);
                     }
+                    const int pos = have + __popc(bal & ((1u << lane) - 1u));
+                    if (ok) {
+                        d[pos] = dk;
+                        id[pos] = ik;
+                    }
+                    have += cnt;
+                    total += cnt;
+                    __syncwarp();
                 }
             }
             if (total < k) {
