@@ -175,7 +175,9 @@ int rbfb_assemble_range(rbfb_ctx* ctx, const rbfb_desc* desc, int first, int cou
 
 /* Ragged stencils in CSR form (ia has nstencils+1 entries), optionally with a
  * per-stencil degree (int8, NULL = desc->degree): the uneven batch. Stencils
- * are bucketed by system size and run in one persistent launch per call,
+ * are bucketed on the device by system size and each bucket runs as one
+ * persistent launch of the kernel shape that fits it. The call is a fixed
+ * launch sequence with no host round trip; on a non-default stream it is
  * captured in a CUDA graph and replayed when the same batch comes again.
  * The Fortran module's fill_kernel (src/rbf_cuda.f90:36-99) is the
  * reference's only CSR-driven assembly. */
