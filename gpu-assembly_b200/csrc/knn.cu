@@ -10,12 +10,13 @@
 //   2. cell of every node on a C x C grid (about kPerCell nodes per cell),
 //      counting sort by cell: cell_start[] and the nodes' coordinates and
 //      indices in cell order (coalesced candidate reads);
-//   3. one warp per query, queries in cell order: gather every node of the
-//      (2R+1)^2 cells around the query's cell into shared memory with its
-//      squared distance, rank the candidates by (squared distance, index)
-//      and keep the k smallest. The result is exact once the k-th distance
-//      is below the distance from the query to the edge of the searched
-//      block; otherwise R grows and the warp searches again. More
+//   3. one warp per query, queries in cell order: walk the nodes of the
+//      (2R+1)^2 cells around the query's cell (their runs of cells laid out
+//      flat over the lanes) and keep, in shared memory with their squared
+//      distances, those closer than the distance from the query to the edge
+//      of the searched block. If at least k are kept, the k nearest nodes
+//      are among them: rank them by (squared distance, index) and write the
+//      k smallest. Otherwise R grows and the warp searches again. More
 //      candidates than the buffer holds are merged chunk by chunk.
 //
 // Distances use the reference's arithmetic exactly: dx*dx + dy*dy of the
