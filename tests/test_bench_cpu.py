@@ -1,0 +1,41 @@
+"""bench.py pieces that run without a GPU: the algorithmic counts the
+roofline uses, the traffic read from the committed ncu summary, and the
+reference arm (the reference's CPU search + the CPU assembly), whose JSON
+line must carry the contract's keys."""
+import json
+import subprocess
+import sys
+
+from conftest import ROOT
+
+sys.path.insert(0, str(ROOT))
+import bench  # noqa: E402
+
+
+def test_algorithmic_counts():
+    n = bench.K + 10  # k + npoly(3)
+    assert bench.N_SYS == n == 45
+    assert bench.FLOP_PER_STENCIL == 2.0 / 3.0 * n ** 3 + 2 * 3 * n ** 2 == 72900.0
+    assert bench.HBM_BYTES_PER_STENCIL == (4 + 16 + 24) * 35 + 16 == 1556
+    assert bench.HBM_COMPULSORY_PER_STENCIL == (4 + 24) * 35 + 20 == 1000
+
+
+def test_traffic_from_the_committed_profile():
+    t = bench.traffic_per_launch("fp64")
+    assert t is not None and 0.3e9 < t < 2e9  # DRAM bytes per full-size launch
+
+
+def test_reference_arm_line():
+    r = subprocess.run([sys.executable, str(ROOT / "bench.py"), "--impl", "reference",
+                        "--steps", "1", "--warmup", "1"], capture_output=True, text=True,
+                       timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    for key in ("metric", "value", "unit", "n_gpus", "steps", "warmup", "ms_per_step",
+                "higher_is_better", "scaling", "vs_baseline", "dtype", "data", "config",
+                "cpu_baseline", "e2e"):
+        assert key in line, key
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["warmup"] >= 3  # the timing rules' minimum
+    assert line["cpu_baseline"]["cores"] >= 1
+    assert line["e2e"]["h2d_bytes_per_step"] == 0
