@@ -259,6 +259,13 @@ __global__ void __launch_bounds__(kWarps * 32) query_kernel(QueryArgs a) {
             R = max(1, (int)ceil(0.5 * (sqrt(want * 1.27) - 1.0)) + 1);
         }
         bool done = false;
+        // First try a tighter radius than the block bound: the distance at
+        // which k + 1 nodes are expected at the grid's mean density (kPerCell
+        // per cell), with a 30% margin. Exactness does not depend on it: if
+        // fewer than k nodes lie inside, the block is walked again with the
+        // full bound.
+        const double est2 = 1.69 * (k + 1) * g.hx * g.hy / (3.141592653589793 * kPerCell);
+        bool tight = true;
         for (int attempt = 0; attempt < 64 && !done; ++attempt) {
             // periodic axes: never more than one period (no cell twice); open
             // axes: up to the whole grid (the clamp below keeps it in range)
@@ -296,12 +303,14 @@ __global__ void __launch_bounds__(kWarps * 32) query_kernel(QueryArgs a) {
             }
             double bound = fmin(bx, by);
             bound = bound * (1.0 - 1e-9) - 1e-15 * fmax(fabs(qx), fabs(qy));
-            // Only candidates inside the circle of radius `bound` (inscribed in
-            // the searched block) are kept: when at least k of them are found,
-            // the k nearest nodes are among them, since every node outside is
-            // farther than all of these; otherwise the block grows. (A block
-            // that covers the whole domain keeps everything.)
+            // Only candidates inside a circle of radius at most `bound`
+            // (inscribed in the searched block) are kept: when at least k of
+            // them are found, the k nearest nodes are among them, since every
+            // node outside is farther than all of these; otherwise the radius
+            // widens to the bound, then the block grows. (A block that covers
+            // the whole domain keeps everything.)
             const double bound2 = bound >= 1e299 ? INFINITY : (bound > 0.0 ? bound * bound : 0.0);
+            const double keep2 = tight ? fmin(bound2, est2) : bound2;
             // gather candidates chunk by chunk; the current best k stay at the front.
             // The block is a list of runs of consecutive cells (one per row, two
             // where a periodic row wraps). A batch of up to 32 runs is laid out
@@ -366,7 +375,7 @@ __global__ void __launch_bounds__(kWarps * 32) query_kernel(QueryArgs a) {
                     int ik = 0;
                     if (ok) {
                         const double d2 = sqdist(qx, qy, a.sx[j], a.sy[j], g.Lx, g.Ly);
-                        ok = d2 < bound2;
+                        ok = d2 < keep2;
                         dk = (unsigned long long)__double_as_longlong(d2);
                         ik = a.sidx[j];
                     }
@@ -416,6 +425,10 @@ __global__ void __launch_bounds__(kWarps * 32) query_kernel(QueryArgs a) {
                 }
             }
             if (total < k) {
+                if (tight && keep2 < bound2) {
+                    tight = false;  // same block, full bound
+                    continue;
+                }
                 R += max(1, R / 2);
                 continue;
             }
