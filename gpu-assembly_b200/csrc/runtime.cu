@@ -268,6 +268,8 @@ const char* rbfb_status_string(int status) {
         case RBFB_ENOTFOUND: return "unknown ticket";
         case RBFB_EBUSY: return "not finished";
         case RBFB_ETOOBIG: return "problem exceeds the fixed scratch of the no-allocation call";
+        case RBFB_ENOCONV: return "iterative solve did not converge within maxit";
+        case RBFB_EBREAKDOWN: return "iterative solve broke down";
         default: return status > 0 ? "singular stencils" : "unknown status";
     }
 }
@@ -301,6 +303,7 @@ int rbfb_create(rbfb_ctx** out, int device) {
 void rbfb_release_pipeline(rbfb_ctx* ctx);  // host_pipeline.cu
 void rbfb_release_knn(rbfb_ctx* ctx);       // knn.cu
 void rbfb_release_batch(rbfb_ctx* ctx);     // batch.cu
+void rbfb_release_solve(rbfb_ctx* ctx);     // solve.cu
 
 int rbfb_destroy(rbfb_ctx* ctx) {
     if (!ctx) return RBFB_OK;
@@ -308,6 +311,7 @@ int rbfb_destroy(rbfb_ctx* ctx) {
     rbfb_release_pipeline(ctx);
     rbfb_release_knn(ctx);
     rbfb_release_batch(ctx);
+    rbfb_release_solve(ctx);
     if (ctx->fb_list) cudaFree(ctx->fb_list);
     if (ctx->ctr) cudaFree(ctx->ctr);
     delete ctx;

@@ -54,6 +54,8 @@ struct rbfb_ctx {
     void* batch = nullptr;
     // host-pipeline staging (pinned) and device buffers
     void* pipe = nullptr;
+    // iterative-solve workspace and its replay graph (solve.cu)
+    void* solve = nullptr;
 };
 
 namespace rbfb {

@@ -29,6 +29,7 @@ LIB_PATH = PKG / "lib" / "librbf_b200.so"
 
 OK, EINVAL, ECUDA, ENOMEM, EUNSUPPORTED, ETIMEOUT, EBUDGET, ENOTFOUND, EBUSY, ETOOBIG = (
     0, -1, -2, -3, -4, -5, -6, -7, -8, -9)
+ENOCONV, EBREAKDOWN = -10, -11  # outcomes of rbfb_solve_bicgstab
 STATIC_MAX_NODES = 65536  # limit of rbfb_knn_stencils_static
 MORTON, HILBERT = 0, 1  # curves of rbfb_curve_keys / rbfb_curve_order
 OP_INTERP, OP_LAPLACE, OP_DX, OP_DY, OP_DXX, OP_DYY, OP_DXY = 1, 2, 4, 8, 16, 32, 64
@@ -100,6 +101,8 @@ _PROTOS = {
     "rbfb_fill_matrices": (_i, [_vp, C.POINTER(Desc), _i, _vp, _vp, _vp, _vp, _vp, _i, _vp]),
     "rbfb_store_to_csr": (_i, [_i, _vp, _vp, _vp, _vp, _vp]),
     "rbfb_spmv": (_i, [_i, _i, _vp, _vp, _vp, _vp, _vp, _i, _vp]),
+    "rbfb_solve_bicgstab": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _i, _vp, _vp, _d, _i,
+                                 C.POINTER(_i), C.POINTER(_d), _vp]),
     "rbfb_curve_keys": (_i, [_vp, _i, _vp, _vp, _vp, _i, _i, _vp, _vp]),
     "rbfb_curve_order": (_i, [_vp, _i, _vp, _vp, _vp, _i, _i, _vp, _vp, _vp, _vp]),
     "rbfb_boundary_last": (_i, [_vp, _i, _vp, _vp, _vp, _vp]),
@@ -244,6 +247,23 @@ class Context:
         st = lib().rbfb_knn_query(self.h, n, _ptr(x), _ptr(y), xq.numel(), _ptr(xq), _ptr(yq),
                                   k, per, _ptr(ja), _stream(stream))
         return self._check(st, "knn_query")
+
+    # ---- solving with an assembled operator
+    def solve_bicgstab(self, values, ja, f, u, k=None, ia=None, bnd=None, tol=1e-10,
+                       maxit=10000, stream=None):
+        """BiCGSTAB for A u = f, A = the stencil operator (fixed width k, or
+        CSR rows ia) with identity rows at bnd; u (float64 device) holds the
+        initial guess and receives the iterate. Returns (status, iters,
+        relres) with status OK, ENOCONV or EBREAKDOWN; raises on errors."""
+        n = f.numel()
+        it, rel = C.c_int(0), C.c_double(0.0)
+        nb = 0 if bnd is None else bnd.numel()
+        st = lib().rbfb_solve_bicgstab(self.h, n, 0 if k is None else k, _ptr(ia), _ptr(ja),
+                                       _ptr(values), _ptr(bnd), nb, _ptr(f), _ptr(u), tol, maxit,
+                                       C.byref(it), C.byref(rel), _stream(stream))
+        if st not in (OK, ENOCONV, EBREAKDOWN):
+            self._check(st, "solve_bicgstab")
+        return st, it.value, rel.value
 
     # ---- assembly
     def assemble(self, desc: Desc, x, y, k, ja, values, info=None, stats=False, stream=None):

@@ -8,6 +8,7 @@ reference's assembly, as the parity tests establish).
     python -m rbf_b200.run --grid 256 --precision mixed --reps 3
     python -m rbf_b200.run --workload disk --precision both
     python -m rbf_b200.run --workload bump --precision both
+    python -m rbf_b200.run --workload disk --precision fp64 --solve 200
 
 Workloads:
   periodic  jittered m x m grid in the periodic unit square (m = --grid),
@@ -19,6 +20,12 @@ Workloads:
             degree 4 (n=79)
 The single-kernel shapes are also what the profiles are captured on (e.g.
 under ncu with ``-k regex:asm_kernel`` on ``--grid 512``).
+
+--solve N (disk only) then runs N BiCGSTAB iterations (tolerance 0, so
+exactly N) on the assembled FP64 Laplacian with identity rows at the
+boundary nodes, for the manufactured solution u = e^x sin 2y + x^2, and
+reports ms per iteration and the algorithmic bytes per iteration
+(solve_bytes) over that time.
 """
 from __future__ import annotations
 
@@ -65,6 +72,16 @@ def _max_rel_err(a, b, ia):
     return worst
 
 
+def solve_bytes(n, nnz):
+    """Algorithmic HBM bytes of one BiCGSTAB iteration of the CUDA solver
+    over n rows and nnz stored weights (ragged CSR): the two operator
+    applications read 12 B per weight (value + column), 4 B of row pointer,
+    1 B of boundary flag and write 8 B per row, and gather their input vector
+    once (8 B per row; 16 B for A s, formed from r and v); the vector passes
+    read rh (8 B), write s and t (16 B), update p (32 B) and u, r (56 B)."""
+    return 24 * nnz + n * (2 * (4 + 1 + 8) + 8 + 8 + 16 + 16 + 32 + 56)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", choices=["periodic", "disk", "bump"], default="periodic")
@@ -75,6 +92,8 @@ def main(argv=None):
     ap.add_argument("--precision", choices=["fp64", "mixed", "both"], default="mixed")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--tune", action="store_true", help="autotune the shape first")
+    ap.add_argument("--solve", type=int, default=0,
+                    help="disk: BiCGSTAB iterations on the assembled Laplacian")
     a = ap.parse_args(argv)
     dev = torch.device("cuda", 0)
     stream = torch.cuda.Stream(dev)  # non-default: the CSR path replays a CUDA graph on it
@@ -114,6 +133,28 @@ def main(argv=None):
                           "bad_info": int((info != 0).sum())}
             out.update(stencils=n, nnz=nnz, k_range=[int(kvec.min()), kmax],
                        degrees=sorted(set(int(v) for v in np.unique(c["degree"]))))
+            if a.solve > 0:
+                L = res[forms[0]][0]  # the Laplacian rows
+                bnd = torch.as_tensor(np.flatnonzero(c["flag"]).astype(np.int32), device=dev)
+                f = -3.0 * torch.exp(xd) * torch.sin(2.0 * yd) + 2.0
+                f[bnd.long()] = (torch.exp(xd) * torch.sin(2.0 * yd) + xd * xd)[bnd.long()]
+                u = torch.zeros(n, dtype=torch.float64, device=dev)
+                ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()  # f and u are made on the default stream
+                with torch.cuda.stream(stream):
+                    ctx.solve_bicgstab(L, ja, f, u, ia=ia, bnd=bnd, tol=0.0, maxit=8,
+                                       stream=stream)  # warm-up: workspace and graph
+                    u.zero_()
+                    ea.record(stream)
+                    st_, it, rel = ctx.solve_bicgstab(L, ja, f, u, ia=ia, bnd=bnd, tol=0.0,
+                                                      maxit=a.solve, stream=stream)
+                    eb.record(stream)
+                torch.cuda.synchronize()
+                ms = ea.elapsed_time(eb)
+                out["solve"] = {"status": R.lib().rbfb_status_string(st_).decode(),
+                                "iterations": it, "relres": rel, "ms": ms,
+                                "ms_per_iteration": ms / max(it, 1),
+                                "algorithmic_GBps": solve_bytes(n, nnz) * it / (ms * 1e-3) / 1e9}
             if len(forms) == 2:
                 out["mixed_max_rel_err_vs_fp64"] = _max_rel_err(res["mixed"], res["fp64"], ia)
         else:

@@ -227,6 +227,33 @@ int rbfb_solve_dp(double* A, int* ipiv, double* B, int* info, void* stream);
 int rbfb_spmv(int n, int k, const int* ja, const double* values, const double* u, double* out,
               const int* bnd, int nbnd, void* stream);
 
+/* ---- solving with the assembled operator ------------------------------------
+ * Solves A u = f by BiCGSTAB (van der Vorst, 1992; no preconditioner). A is
+ * the operator rbfb_spmv applies: the stencil rows (fixed width k when ia is
+ * NULL, else the CSR rows ja[ia[s] .. ia[s+1])) with the nbnd rows listed in
+ * bnd replaced by identity rows, so that f holds the boundary values there.
+ * The reference builds this operator as mv_op and leaves the solve after it
+ * empty (src/main.cpp:57-68). Every ja entry must lie in [0, n).
+ *
+ * u holds the initial guess on entry and the last iterate on exit. The
+ * iteration stops when the recursive residual satisfies
+ * ||r||_2 <= tol * ||f||_2, after maxit iterations, or on a breakdown (a
+ * zero or non-finite denominator). When f = 0, u is set to zero.
+ * Synchronous on `stream`. Returns RBFB_OK when converged, RBFB_ENOCONV when
+ * maxit ran out, RBFB_EBREAKDOWN on a breakdown, a negative argument or CUDA
+ * code otherwise. *iters_h and *relres_h (host, either may be NULL) receive
+ * the iterations taken and ||r||_2 / ||f||_2.
+ *
+ * The sums are deterministic: one thread per row, fused multiply-adds in row
+ * order, and dot products reduced in a fixed order over a grid of
+ * min(ceil(n / 256), 8 * SMs) blocks of 256 threads. */
+#define RBFB_ENOCONV (-10)    /* iterative solve: maxit ran out              */
+#define RBFB_EBREAKDOWN (-11) /* iterative solve: zero or non-finite pivot   */
+int rbfb_solve_bicgstab(rbfb_ctx* ctx, int n, int k, const int* ia, const int* ja,
+                        const double* values, const int* bnd, int nbnd, const double* f,
+                        double* u, double tol, int maxit, int* iters_h, double* relres_h,
+                        void* stream);
+
 /* ---- node renumbering (locality) ------------------------------------------
  * A permutation is stored in gather form, as the reference's
  * rbf::Permutation (src/rbf_reorder.h:68-80): perm[i] is the OLD index of

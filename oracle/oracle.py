@@ -67,6 +67,12 @@ def lib():
                                             C.c_void_p]
         L.orc_spmv.restype = None
         L.orc_spmv.argtypes = [C.c_int, C.c_int, _ip, _dp, _dp, _dp, C.c_void_p, C.c_int]
+        L.orc_solve_grid.restype = C.c_int
+        L.orc_solve_grid.argtypes = [C.c_int, C.c_int]
+        L.orc_bicgstab.restype = C.c_int
+        L.orc_bicgstab.argtypes = [C.c_int, C.c_int, C.c_void_p, _ip, _dp, C.c_void_p, C.c_int,
+                                   _dp, _dp, C.c_double, C.c_int, C.c_int,
+                                   C.POINTER(C.c_int), C.POINTER(C.c_double)]
         L.orc_curve_keys.restype = C.c_int
         L.orc_curve_keys.argtypes = [C.c_int, _dp, _dp, C.c_void_p, C.c_int, C.c_int,
                                      np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")]
@@ -287,6 +293,30 @@ def spmv(ja, values, u, k, bnd=None):
     lib().orc_spmv(n, k, ja, values, u, out, None if b is None else b.ctypes.data,
                    0 if b is None else b.size)
     return out
+
+
+def solve_grid(n, sms):
+    """Blocks of the CUDA solver's reductions for n rows on `sms` SMs."""
+    return lib().orc_solve_grid(n, sms)
+
+
+def bicgstab(values, ja, f, u0, k=None, ia=None, bnd=None, tol=1e-10, maxit=10000, grid=1):
+    """BiCGSTAB with the CUDA solver's summation order for a grid of `grid`
+    blocks. Returns (status, u, iters, relres); status 0, -10 (maxit) or
+    -11 (breakdown); ValueError on bad arguments."""
+    values, ja, f = _f64(values), _i32(ja), _f64(f)
+    u = _f64(u0).copy()
+    n = f.size
+    iaa = None if ia is None else _i32(ia)
+    b = None if bnd is None else _i32(bnd)
+    it, rel = C.c_int(0), C.c_double(0.0)
+    st = lib().orc_bicgstab(n, 0 if k is None else k, None if iaa is None else iaa.ctypes.data,
+                            ja, values, None if b is None else b.ctypes.data,
+                            0 if b is None else b.size, f, u, tol, maxit, grid, C.byref(it),
+                            C.byref(rel))
+    if st == -1:
+        raise ValueError("bad bicgstab arguments")
+    return st, u, it.value, rel.value
 
 
 MORTON, HILBERT = 0, 1

@@ -778,3 +778,150 @@ extern "C" void orc_renumber_csr(int n, const int* ia, const int* ja, const int*
         ia_out[i + 1] = ia_out[i] + (b - a);
     }
 }
+
+// ---- iterative solve ---------------------------------------------------------------
+// BiCGSTAB (van der Vorst, 1992) on the operator orc_spmv applies: stencil
+// rows (fixed width k, or CSR rows when ia is given) with identity rows at
+// the boundary list; the solve the reference leaves after building that
+// operator (src/main.cpp:57-68). Every sum is taken in the order the CUDA
+// solver takes it, so results agree bit for bit: rows in fused
+// multiply-adds from zero; thread T = b * 256 + t of a grid of `grid` blocks
+// owns rows T, T + 256 * grid, ... in ascending order; a warp sums by an
+// xor butterfly over rounds 16, 8, 4, 2, 1; a block by the butterfly over
+// its 8 warp sums (lanes 8..31 zero); the grid by thread t adding the
+// partials of blocks t, t + 256, ... and the block butterfly of those.
+// Returns 0 (converged), -10 (maxit reached), -11 (breakdown) or -1 (bad
+// argument), as rbfb_solve_bicgstab.
+namespace {
+
+double butterfly32(double* v) {
+    double t[32];
+    for (int o = 16; o; o >>= 1) {
+        for (int l = 0; l < 32; ++l) t[l] = v[l] + v[l ^ o];
+        for (int l = 0; l < 32; ++l) v[l] = t[l];
+    }
+    return v[0];
+}
+
+double block_butterfly(const double* th) {  // 256 thread values
+    double lanes[32], ws[8];
+    for (int w = 0; w < 8; ++w) {
+        for (int l = 0; l < 32; ++l) lanes[l] = th[w * 32 + l];
+        ws[w] = butterfly32(lanes);
+    }
+    for (int l = 0; l < 32; ++l) lanes[l] = l < 8 ? ws[l] : 0.0;
+    return butterfly32(lanes);
+}
+
+struct SolveSums {
+    int n, grid;
+    std::vector<double> th, part, g;
+    SolveSums(int n_, int grid_)
+        : n(n_), grid(grid_), th(static_cast<size_t>(grid_) * 256), part(grid_), g(256) {}
+    double dot(const double* x, const double* y) {
+        std::fill(th.begin(), th.end(), 0.0);
+        const size_t nt = th.size();
+        for (size_t s = 0; s < static_cast<size_t>(n); ++s) th[s % nt] = std::fma(x[s], y[s], th[s % nt]);
+        for (int b = 0; b < grid; ++b) part[b] = block_butterfly(&th[static_cast<size_t>(b) * 256]);
+        for (int t = 0; t < 256; ++t) {
+            double a = 0.0;
+            for (int b = t; b < grid; b += 256) a += part[b];
+            g[t] = a;
+        }
+        return block_butterfly(g.data());
+    }
+};
+
+template <class W>
+double apply_row(int s, int k, const int* ia, const int* ja, const double* values,
+                 const std::vector<unsigned char>& bflag, W w) {
+    if (bflag[s]) return w(s);
+    const long long b = ia ? ia[s] : static_cast<long long>(s) * k;
+    const long long e = ia ? ia[s + 1] : b + k;
+    double acc = 0.0;
+    for (long long q = b; q < e; ++q) acc = std::fma(values[q], w(ja[q]), acc);
+    return acc;
+}
+
+}  // namespace
+
+extern "C" int orc_solve_grid(int n, int sms) {
+    const long long want = (static_cast<long long>(n) + 255) / 256;
+    return static_cast<int>(std::max(1LL, std::min(want, 8LL * sms)));
+}
+
+extern "C" int orc_bicgstab(int n, int k, const int* ia, const int* ja, const double* values,
+                            const int* bnd, int nbnd, const double* f, double* u, double tol,
+                            int maxit, int grid, int* iters, double* relres) {
+    *iters = 0;
+    *relres = 0.0;
+    if (n < 0 || nbnd < 0 || maxit < 0 || !(tol >= 0.0) || !std::isfinite(tol) || (!ia && k < 1) ||
+        grid < 1)
+        return -1;
+    if (n == 0) return 0;
+    std::vector<unsigned char> bflag(n, 0);
+    for (int b = 0; b < nbnd; ++b) {
+        if (bnd[b] < 0 || bnd[b] >= n) return -1;
+        bflag[bnd[b]] = 1;
+    }
+    const size_t N = n;
+    std::vector<double> r(N), rh(N), p(N, 0.0), v(N, 0.0), s(N), t(N);
+    SolveSums sums(n, grid);
+    for (int i = 0; i < n; ++i) {
+        r[i] = f[i] - apply_row(i, k, ia, ja, values, bflag, [u](int j) { return u[j]; });
+        rh[i] = r[i];
+    }
+    double rr = sums.dot(r.data(), r.data());
+    const double ff = sums.dot(f, f);
+    const double thresh2 = tol * tol * ff;
+    auto finish = [&](int code) {
+        *relres = ff > 0.0 ? std::sqrt(rr / ff) : 0.0;
+        return code;
+    };
+    if (!std::isfinite(rr) || !std::isfinite(ff)) return finish(-11);
+    if (rr <= thresh2) return finish(0);
+    if (ff == 0.0) {
+        std::fill(u, u + n, 0.0);
+        return 0;
+    }
+    if (maxit <= 0) return finish(-10);
+    double rho = rr, alpha = 1.0, omega = 1.0, beta = 0.0;
+    int iter = 0;
+    for (;;) {
+        for (int i = 0; i < n; ++i) p[i] = std::fma(beta, std::fma(-omega, v[i], p[i]), r[i]);
+        for (int i = 0; i < n; ++i)
+            v[i] = apply_row(i, k, ia, ja, values, bflag, [&p](int j) { return p[j]; });
+        const double sigma = sums.dot(rh.data(), v.data());
+        if (sigma == 0.0 || !std::isfinite(sigma)) return finish(-11);
+        alpha = rho / sigma;
+        for (int i = 0; i < n; ++i) s[i] = std::fma(-alpha, v[i], r[i]);
+        for (int i = 0; i < n; ++i)
+            t[i] = apply_row(i, k, ia, ja, values, bflag, [&s](int j) { return s[j]; });
+        const double ts = sums.dot(t.data(), s.data());
+        const double tt = sums.dot(t.data(), t.data());
+        const double ss = sums.dot(s.data(), s.data());
+        bool pending = false;
+        if (ss <= thresh2) {
+            omega = 0.0;
+        } else if (tt == 0.0 || !std::isfinite(tt) || !std::isfinite(ts)) {
+            omega = 0.0;
+            pending = true;
+        } else {
+            omega = ts / tt;
+        }
+        for (int i = 0; i < n; ++i) {
+            u[i] = std::fma(omega, s[i], std::fma(alpha, p[i], u[i]));
+            r[i] = std::fma(-omega, t[i], s[i]);
+        }
+        const double rho_new = sums.dot(rh.data(), r.data());
+        rr = sums.dot(r.data(), r.data());
+        *iters = ++iter;
+        if (!std::isfinite(rr)) return finish(-11);
+        if (rr <= thresh2) return finish(0);
+        if (pending || omega == 0.0) return finish(-11);
+        if (iter >= maxit) return finish(-10);
+        if (rho_new == 0.0 || !std::isfinite(rho_new)) return finish(-11);
+        beta = (rho_new / rho) * (alpha / omega);
+        rho = rho_new;
+    }
+}
