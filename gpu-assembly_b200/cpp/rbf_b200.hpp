@@ -17,6 +17,9 @@
 //   rbf_b200::laplace_config / assemble_laplace_weights
 //                                              the Laplacian assembly src/main.cpp:15-16,44-45
 //                                              sketches (never implemented there)
+//   rbf_b200::StencilOperator                  mv_op of src/main.cpp:57-66 (A.spmv, then the
+//                                              boundary fix) and, as solve(), the solve that
+//                                              src/main.cpp:68 leaves empty (BiCGSTAB)
 //
 // T = double assembles in FP64; rbf_b200::Precision lets a caller ask for
 // the FP32-factorisation + FP64-refinement form instead (weights are FP64
@@ -199,6 +202,44 @@ void assemble_laplace_weights(int npoints, const typename Config::value_type* x,
     check(rbfb_assemble(context(), &d, npoints, x, y, Config::N, ja, A_tab, info, nullptr, stream),
           "assemble_laplace_weights");
 }
+
+// The assembled operator with identity rows at the boundary nodes, on device
+// arrays: operator() is mv_op (y = A x, then y[bnd] = x[bnd]); solve() runs
+// BiCGSTAB for A u = f from the guess in u to ||f - A u|| <= tol ||f|| and
+// returns the iterations taken, throwing on argument or CUDA errors and,
+// unless allow_unconverged, when maxit runs out or the method breaks down.
+// ia == nullptr selects fixed-width rows of k (the reference's layout,
+// src/rbf_operators.h:307-313); operator() needs that layout.
+struct StencilOperator {
+    int n = 0;
+    int k = 0;
+    const int* ja = nullptr;
+    const double* values = nullptr;
+    const int* bnd = nullptr;
+    int nbnd = 0;
+    const int* ia = nullptr;
+
+    void operator()(const double* x, double* y, cudaStream_t stream = nullptr) const {
+        if (ia) throw std::runtime_error("rbf_b200: mv_op needs fixed-width rows");
+        check(rbfb_spmv(n, k, ja, values, x, y, bnd, nbnd, stream), "mv_op");
+    }
+
+    int solve(const double* f, double* u, double tol = 1e-10, int maxit = 10000,
+              double* relres = nullptr, bool allow_unconverged = false,
+              cudaStream_t stream = nullptr) const {
+        int iters = 0;
+        double rel = 0.0;
+        const int st = rbfb_solve_bicgstab(context(), n, k, ia, ja, values, bnd, nbnd, f, u, tol,
+                                           maxit, &iters, &rel, stream);
+        if (relres) *relres = rel;
+        if (st == RBFB_ENOCONV || st == RBFB_EBREAKDOWN) {
+            if (!allow_unconverged) check(st, "solve");
+        } else {
+            check(st, "solve");
+        }
+        return iters;
+    }
+};
 
 }  // namespace rbf_b200
 

@@ -48,6 +48,7 @@ module rbf_b200
 
   public :: rbfb_create, rbfb_destroy, rbfb_knn_stencils, rbfb_assemble, rbfb_assemble_csr
   public :: rbfb_fill_matrices, rbfb_store_to_csr, rbfb_solve_dp, rbfb_spmv
+  public :: rbfb_solve_bicgstab
 
   interface
     integer(c_int) function rbfb_create(ctx, device) bind(c, name="rbfb_create")
@@ -118,6 +119,18 @@ module rbf_b200
       import :: c_int, c_ptr
       integer(c_int), value :: n, k, nbnd
       type(c_ptr), value :: ja, values, u, out, bnd, stream
+    end function
+
+    ! BiCGSTAB for A u = f with that operator: the solve src/main.cpp:68 leaves
+    ! empty. ia = c_null_ptr selects fixed-width rows of k.
+    integer(c_int) function rbfb_solve_bicgstab(ctx, n, k, ia, ja, values, bnd, nbnd, f, u, &
+        tol, maxit, iters, relres, stream) bind(c, name="rbfb_solve_bicgstab")
+      import :: c_int, c_ptr, c_double
+      type(c_ptr), value :: ctx, ia, ja, values, bnd, f, u, stream
+      integer(c_int), value :: n, k, nbnd, maxit
+      real(c_double), value :: tol
+      integer(c_int), intent(out) :: iters
+      real(c_double), intent(out) :: relres
     end function
   end interface
 end module rbf_b200

@@ -97,6 +97,9 @@ int main() {
                                                   nullptr, nullptr);
         rbf_b200::NodeSet<> ns({0.0}, {0.0}, {0});
         (void)ns.stencils(1);
+        rbf_b200::StencilOperator op;
+        op(nullptr, nullptr);
+        (void)op.solve(nullptr, nullptr);
     }
     return st == RBFB_ECUDA ? 0 : 1;
 }

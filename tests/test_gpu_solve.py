@@ -110,10 +110,12 @@ def test_solve_edge_cases(ctx, torch_cuda):
                                                          bnd=bnd, tol=1e-14, maxit=3)
     assert st == R.ENOCONV and ost == -10 and it == oit == 3 and rel == orel
     np.testing.assert_array_equal(u, ou)
-    # a converged guess takes no iteration and is returned unchanged
-    (st, it, rel), u, _ = _solve_both(ctx, T, L, ja, f, ou, k=k, bnd=bnd, tol=1.0)
+    # a guess that already meets the tolerance takes no iteration and is
+    # returned unchanged
+    _, us, _, _ = O.bicgstab(L, ja, f, np.zeros(n), k=k, bnd=bnd, tol=1e-12)
+    (st, it, rel), u, _ = _solve_both(ctx, T, L, ja, f, us, k=k, bnd=bnd, tol=1e-9)
     assert st == R.OK and it == 0
-    np.testing.assert_array_equal(u, ou)
+    np.testing.assert_array_equal(u, us)
     # an out-of-range boundary index is an argument error and leaves u alone
     ud = _dev(T, np.full(n, 7.0))
     with pytest.raises(R.RbfError):
