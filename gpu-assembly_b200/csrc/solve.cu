@@ -13,14 +13,18 @@
 //           stop when (r, r) <= tol^2 (f, f); beta = ((rh, r) / rho) (alpha / omega)
 //
 // On this part the iteration is HBM-bound: each step reads the operator
-// (12 B per stored weight, twice) and a handful of vectors. It is laid out
-// as four kernels per iteration, each one pass over the rows:
+// (12 B per stored weight, twice) and a handful of vectors. The operator
+// passes stream each block's rows through shared memory in coalesced
+// stretches (a tile of 256 rows is one contiguous range of stored weights)
+// and each thread then sums its own row from there, in row order. It is laid
+// out as five kernels per iteration, each one pass over the rows:
 //   p_kernel       p = r + beta (p - omega v)
 //   spmv_v_kernel  v = A p, with the partial sums of (rh, v)
-//   spmv_t_kernel  s = r - alpha v, t = A s (s formed at the gather, so it
-//                  is never written and re-read before the product), with
-//                  the partial sums of (t, s), (t, t), (s, s)
+//   s_kernel       s = r - alpha v
+//   spmv_t_kernel  t = A s, with the partial sums of (t, s), (t, t), (s, s)
 //   update_kernel  u += alpha p + omega s, r = s - omega t, with (rh, r), (r, r)
+// s gets a pass of its own so that A s gathers one vector per stored weight
+// rather than forming s from two gathered ones (r and v).
 // The scalars live in device memory: the block that finishes a kernel last
 // (an atomic arrival count, no waiting) adds the blocks' partial sums in
 // block order and computes the next coefficients and the stop flag, which
@@ -33,7 +37,7 @@
 // thread's rows (grid stride) in ascending order; a warp by an xor
 // butterfly (16, 8, 4, 2, 1); a block by the butterfly over its warps'
 // sums; the grid by thread t summing the partials of blocks t, t + 256, ...
-// then the block butterfly. The grid is min(ceil(n / 256), 8 * SMs) blocks.
+// then the block butterfly. The grid is min(ceil(n / 256), 6 * SMs) blocks.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -49,6 +53,11 @@ namespace solve {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kChunk = 8;  // iterations between two looks at the stop flag
+constexpr int kStage = 1024;  // stored weights per shared-memory stretch
+// Blocks per SM that stay resident together (40 registers and 12.5 KB of
+// shared memory each); the grid is that many per SM, so none waits for a
+// second wave.
+constexpr int kBlocksPerSm = 6;
 
 enum : int { RUNNING = 0, CONVERGED = 1, MAXIT = 2, BREAKDOWN = 3, ZERO_RHS = 4, BAD_INPUT = 5 };
 
@@ -86,21 +95,56 @@ struct Workspace {
     long long graph_launches = 0;
 };
 
-// (A w)_s: row s of the operator applied to the vector w(j), j < n.
+// Weights and columns of one stretch of a row tile, staged in shared memory.
+struct Stage {
+    double v[kStage];
+    int j[kStage];
+};
+
+// (A w)_s for the row s = r0 + threadIdx.x of the block's tile of rows
+// [r0, r0 + kThreads) (rows past n take no part), w(j) the vector applied.
+// The tile's rows are one contiguous range of stored weights, so the block
+// streams it through shared memory in coalesced stretches of kStage; each
+// thread then adds its own row from there in row order, the same sums as a
+// plain row-by-row product. Every thread of the block must call this with
+// the same r0 (it holds barriers).
 template <class W>
-__device__ __forceinline__ double apply_row(const Args& a, int s, W w) {
-    if (a.bflag[s]) return w(s);
-    long long b, e;
+__device__ __forceinline__ double apply_tile(const Args& a, long long r0, Stage& sm, W w) {
+    const long long s = r0 + threadIdx.x;
+    const long long rend = (a.n - r0 < kThreads) ? a.n : r0 + kThreads;
+    long long lo, hi, b = 0, e = 0;
     if (a.ia) {
-        b = __ldg(a.ia + s);
-        e = __ldg(a.ia + s + 1);
+        lo = __ldg(a.ia + r0);
+        hi = __ldg(a.ia + rend);
+        if (s < a.n) {
+            b = __ldg(a.ia + s);
+            e = __ldg(a.ia + s + 1);
+        }
     } else {
-        b = static_cast<long long>(s) * a.k;
+        lo = r0 * a.k;
+        hi = rend * a.k;
+        b = s * a.k;
         e = b + a.k;
     }
+    const bool boundary = s < a.n && a.bflag[s];
+    const bool own = s < a.n && !boundary;
     double acc = 0.0;
-    for (long long q = b; q < e; ++q) acc = fma(__ldg(a.values + q), w(__ldg(a.ja + q)), acc);
-    return acc;
+    for (long long base = lo; base < hi; base += kStage) {
+        const int cnt = static_cast<int>(hi - base < kStage ? hi - base : kStage);
+        for (int i = threadIdx.x; i < cnt; i += kThreads) {
+            sm.v[i] = __ldg(a.values + base + i);
+            sm.j[i] = __ldg(a.ja + base + i);
+        }
+        __syncthreads();
+        if (own) {
+            const long long q0 = b > base ? b : base;
+            const long long q1 = e < base + cnt ? e : base + cnt;
+            for (long long q = q0; q < q1; ++q)
+                acc = fma(sm.v[q - base], w(sm.j[q - base]), acc);
+        }
+        __syncthreads();
+    }
+    return boundary ? w(static_cast<int>(s)) : acc;
 }
 
 // Sums NV values over the block; the totals end up in every lane of warp 0.
@@ -168,12 +212,15 @@ __global__ void flag_kernel(int n, int nb, const int* __restrict__ bnd, unsigned
 }
 
 // r = f - A u, rh = r, p = v = 0; rho = (r, r), ff = (f, f).
-__global__ void __launch_bounds__(kThreads) init_kernel(Args a, double tol, int maxit) {
+__global__ void __launch_bounds__(kThreads, kBlocksPerSm) init_kernel(Args a, double tol, int maxit) {
+    __shared__ Stage sm;
     double acc[2] = {0.0, 0.0};
-    const int stride = gridDim.x * kThreads;
-    for (int s = blockIdx.x * kThreads + threadIdx.x; s < a.n; s += stride) {
-        const double* u = a.u;
-        const double au = apply_row(a, s, [u](int j) { return u[j]; });
+    const long long stride = static_cast<long long>(gridDim.x) * kThreads;
+    const double* u = a.u;
+    for (long long r0 = static_cast<long long>(blockIdx.x) * kThreads; r0 < a.n; r0 += stride) {
+        const double au = apply_tile(a, r0, sm, [u](int j) { return u[j]; });
+        const long long s = r0 + threadIdx.x;
+        if (s >= a.n) continue;
         const double fs = a.f[s];
         const double r = fs - au;
         a.r[s] = r;
@@ -211,7 +258,7 @@ __global__ void __launch_bounds__(kThreads) init_kernel(Args a, double tol, int 
     st->arrive = 0;
 }
 
-__global__ void __launch_bounds__(kThreads) p_kernel(Args a) {
+__global__ void __launch_bounds__(kThreads, kBlocksPerSm) p_kernel(Args a) {
     const State* st = a.st;
     if (st->done) return;
     const double beta = st->beta, omega = st->omega;
@@ -220,14 +267,17 @@ __global__ void __launch_bounds__(kThreads) p_kernel(Args a) {
         a.p[s] = fma(beta, fma(-omega, a.v[s], a.p[s]), a.r[s]);
 }
 
-__global__ void __launch_bounds__(kThreads) spmv_v_kernel(Args a) {
+__global__ void __launch_bounds__(kThreads, kBlocksPerSm) spmv_v_kernel(Args a) {
     State* st = a.st;
     if (st->done) return;
+    __shared__ Stage sm;
     double acc[1] = {0.0};
-    const int stride = gridDim.x * kThreads;
+    const long long stride = static_cast<long long>(gridDim.x) * kThreads;
     const double* p = a.p;
-    for (int s = blockIdx.x * kThreads + threadIdx.x; s < a.n; s += stride) {
-        const double v = apply_row(a, s, [p](int j) { return __ldg(p + j); });
+    for (long long r0 = static_cast<long long>(blockIdx.x) * kThreads; r0 < a.n; r0 += stride) {
+        const double v = apply_tile(a, r0, sm, [p](int j) { return __ldg(p + j); });
+        const long long s = r0 + threadIdx.x;
+        if (s >= a.n) continue;
         a.v[s] = v;
         acc[0] = fma(a.rh[s], v, acc[0]);
     }
@@ -241,19 +291,27 @@ __global__ void __launch_bounds__(kThreads) spmv_v_kernel(Args a) {
     st->arrive = 0;
 }
 
-__global__ void __launch_bounds__(kThreads) spmv_t_kernel(Args a) {
-    State* st = a.st;
+__global__ void __launch_bounds__(kThreads, kBlocksPerSm) s_kernel(Args a) {
+    const State* st = a.st;
     if (st->done) return;
     const double alpha = st->alpha;
-    double acc[3] = {0.0, 0.0, 0.0};
     const int stride = gridDim.x * kThreads;
-    const double* r = a.r;
-    const double* v = a.v;
-    for (int i = blockIdx.x * kThreads + threadIdx.x; i < a.n; i += stride) {
-        const double si = fma(-alpha, v[i], r[i]);
-        const double ti =
-            apply_row(a, i, [r, v, alpha](int j) { return fma(-alpha, __ldg(v + j), __ldg(r + j)); });
-        a.s[i] = si;
+    for (int i = blockIdx.x * kThreads + threadIdx.x; i < a.n; i += stride)
+        a.s[i] = fma(-alpha, a.v[i], a.r[i]);
+}
+
+__global__ void __launch_bounds__(kThreads, kBlocksPerSm) spmv_t_kernel(Args a) {
+    State* st = a.st;
+    if (st->done) return;
+    __shared__ Stage sm;
+    double acc[3] = {0.0, 0.0, 0.0};
+    const long long stride = static_cast<long long>(gridDim.x) * kThreads;
+    const double* sv = a.s;
+    for (long long r0 = static_cast<long long>(blockIdx.x) * kThreads; r0 < a.n; r0 += stride) {
+        const double ti = apply_tile(a, r0, sm, [sv](int j) { return __ldg(sv + j); });
+        const long long i = r0 + threadIdx.x;
+        if (i >= a.n) continue;
+        const double si = sv[i];
         a.t[i] = ti;
         acc[0] = fma(ti, si, acc[0]);
         acc[1] = fma(ti, ti, acc[1]);
@@ -272,7 +330,7 @@ __global__ void __launch_bounds__(kThreads) spmv_t_kernel(Args a) {
     st->arrive = 0;
 }
 
-__global__ void __launch_bounds__(kThreads) update_kernel(Args a) {
+__global__ void __launch_bounds__(kThreads, kBlocksPerSm) update_kernel(Args a) {
     State* st = a.st;
     if (st->done) return;
     const double alpha = st->alpha, omega = st->omega;
@@ -312,7 +370,7 @@ __global__ void __launch_bounds__(kThreads) update_kernel(Args a) {
 
 int grid_of(const rbfb_ctx* ctx, int n) {
     const long long want = (static_cast<long long>(n) + kThreads - 1) / kThreads;
-    return static_cast<int>(std::max(1LL, std::min(want, 8LL * ctx->sms)));
+    return static_cast<int>(std::max(1LL, std::min(want, 1LL * kBlocksPerSm * ctx->sms)));
 }
 
 void release(Workspace* w) {
@@ -364,14 +422,15 @@ int ensure(rbfb_ctx* ctx, int n, int grid) {
     return RBFB_OK;
 }
 
-// Enqueues kChunk iterations (4 launches each).
+// Enqueues kChunk iterations (5 launches each).
 int enqueue_chunk(rbfb_ctx* ctx, const Args& a, int grid, cudaStream_t st) {
     for (int it = 0; it < kChunk; ++it) {
         p_kernel<<<grid, kThreads, 0, st>>>(a);
         spmv_v_kernel<<<grid, kThreads, 0, st>>>(a);
+        s_kernel<<<grid, kThreads, 0, st>>>(a);
         spmv_t_kernel<<<grid, kThreads, 0, st>>>(a);
         update_kernel<<<grid, kThreads, 0, st>>>(a);
-        ctx->launches += 4;
+        ctx->launches += 5;
     }
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? RBFB_OK : cuda_fail(ctx, e, "solve kernels");

@@ -77,9 +77,9 @@ def solve_bytes(n, nnz):
     over n rows and nnz stored weights (ragged CSR): the two operator
     applications read 12 B per weight (value + column), 4 B of row pointer,
     1 B of boundary flag and write 8 B per row, and gather their input vector
-    once (8 B per row; 16 B for A s, formed from r and v); the vector passes
-    read rh (8 B), write s and t (16 B), update p (32 B) and u, r (56 B)."""
-    return 24 * nnz + n * (2 * (4 + 1 + 8) + 8 + 8 + 16 + 16 + 32 + 56)
+    (p, s) once (8 B per row each); the vector passes read rh (8 B), form s
+    from r and v (24 B), update p (32 B) and u, r (56 B)."""
+    return 24 * nnz + n * (2 * (4 + 1 + 8) + 8 + 8 + 8 + 24 + 32 + 56)
 
 
 def main(argv=None):

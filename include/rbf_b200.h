@@ -246,7 +246,7 @@ int rbfb_spmv(int n, int k, const int* ja, const double* values, const double* u
  *
  * The sums are deterministic: one thread per row, fused multiply-adds in row
  * order, and dot products reduced in a fixed order over a grid of
- * min(ceil(n / 256), 8 * SMs) blocks of 256 threads. */
+ * min(ceil(n / 256), 6 * SMs) blocks of 256 threads. */
 #define RBFB_ENOCONV (-10)    /* iterative solve: maxit ran out              */
 #define RBFB_EBREAKDOWN (-11) /* iterative solve: zero or non-finite pivot   */
 int rbfb_solve_bicgstab(rbfb_ctx* ctx, int n, int k, const int* ia, const int* ja,

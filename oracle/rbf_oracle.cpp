@@ -847,7 +847,7 @@ double apply_row(int s, int k, const int* ia, const int* ja, const double* value
 
 extern "C" int orc_solve_grid(int n, int sms) {
     const long long want = (static_cast<long long>(n) + 255) / 256;
-    return static_cast<int>(std::max(1LL, std::min(want, 8LL * sms)));
+    return static_cast<int>(std::max(1LL, std::min(want, 6LL * sms)));
 }
 
 extern "C" int orc_bicgstab(int n, int k, const int* ia, const int* ja, const double* values,

@@ -110,7 +110,7 @@ def test_grid_and_identity_operator():
     rng = np.random.default_rng(0)
     for n in (1, 255, 256, 257, 10_000, 300_001):
         for sms in (1, 148):
-            assert O.solve_grid(n, sms) == max(1, min((n + 255) // 256, 8 * sms))
+            assert O.solve_grid(n, sms) == max(1, min((n + 255) // 256, 6 * sms))
         f = rng.standard_normal(n)
         st, u, it, rel = O.bicgstab(np.zeros(0), np.zeros(0, np.int32), f, np.zeros(n),
                                     ia=np.zeros(n + 1, np.int32), bnd=np.arange(n, dtype=np.int32),
