@@ -13,11 +13,10 @@
 //           stop when (r, r) <= tol^2 (f, f); beta = ((rh, r) / rho) (alpha / omega)
 //
 // On this part the iteration is HBM-bound: each step reads the operator
-// (12 B per stored weight, twice) and a handful of vectors. The operator
-// passes stream each block's rows through shared memory in coalesced
-// stretches (a tile of 256 rows is one contiguous range of stored weights)
-// and each thread then sums its own row from there, in row order. It is laid
-// out as five kernels per iteration, each one pass over the rows:
+// (12 B per stored weight, twice) and a handful of vectors; the operator
+// passes are bound by their gathers, each thread summing its own row in row
+// order with eight gathers in flight. It is laid out as five kernels per
+// iteration, each one pass over the rows:
 //   p_kernel       p = r + beta (p - omega v)
 //   spmv_v_kernel  v = A p, with the partial sums of (rh, v)
 //   s_kernel       s = r - alpha v
@@ -53,10 +52,8 @@ namespace solve {
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
 constexpr int kChunk = 8;  // iterations between two looks at the stop flag
-constexpr int kStage = 1024;  // stored weights per shared-memory stretch
-// Blocks per SM that stay resident together (40 registers and 12.5 KB of
-// shared memory each); the grid is that many per SM, so none waits for a
-// second wave.
+// Blocks per SM that stay resident together (at most 40 registers a
+// thread); the grid is that many per SM, so none waits for a second wave.
 constexpr int kBlocksPerSm = 6;
 
 enum : int { RUNNING = 0, CONVERGED = 1, MAXIT = 2, BREAKDOWN = 3, ZERO_RHS = 4, BAD_INPUT = 5 };
@@ -95,56 +92,37 @@ struct Workspace {
     long long graph_launches = 0;
 };
 
-// Weights and columns of one stretch of a row tile, staged in shared memory.
-struct Stage {
-    double v[kStage];
-    int j[kStage];
-};
-
-// (A w)_s for the row s = r0 + threadIdx.x of the block's tile of rows
-// [r0, r0 + kThreads) (rows past n take no part), w(j) the vector applied.
-// The tile's rows are one contiguous range of stored weights, so the block
-// streams it through shared memory in coalesced stretches of kStage; each
-// thread then adds its own row from there in row order, the same sums as a
-// plain row-by-row product. Every thread of the block must call this with
-// the same r0 (it holds barriers).
+// (A w)_s: row s of the operator applied to the vector w(j), j < n, summed
+// in row order. The loop takes the row eight weights at a time, with the
+// eight weights, columns and gathered entries loaded before the eight fused
+// multiply-adds, so each thread has eight independent gathers in flight
+// instead of one (the sums are the same as a one-at-a-time loop).
 template <class W>
-__device__ __forceinline__ double apply_tile(const Args& a, long long r0, Stage& sm, W w) {
-    const long long s = r0 + threadIdx.x;
-    const long long rend = (a.n - r0 < kThreads) ? a.n : r0 + kThreads;
-    long long lo, hi, b = 0, e = 0;
+__device__ __forceinline__ double apply_row(const Args& a, long long s, W w) {
+    if (a.bflag[s]) return w(static_cast<int>(s));
+    long long q, e;
     if (a.ia) {
-        lo = __ldg(a.ia + r0);
-        hi = __ldg(a.ia + rend);
-        if (s < a.n) {
-            b = __ldg(a.ia + s);
-            e = __ldg(a.ia + s + 1);
-        }
+        q = __ldg(a.ia + s);
+        e = __ldg(a.ia + s + 1);
     } else {
-        lo = r0 * a.k;
-        hi = rend * a.k;
-        b = s * a.k;
-        e = b + a.k;
+        q = s * a.k;
+        e = q + a.k;
     }
-    const bool boundary = s < a.n && a.bflag[s];
-    const bool own = s < a.n && !boundary;
     double acc = 0.0;
-    for (long long base = lo; base < hi; base += kStage) {
-        const int cnt = static_cast<int>(hi - base < kStage ? hi - base : kStage);
-        for (int i = threadIdx.x; i < cnt; i += kThreads) {
-            sm.v[i] = __ldg(a.values + base + i);
-            sm.j[i] = __ldg(a.ja + base + i);
-        }
-        __syncthreads();
-        if (own) {
-            const long long q0 = b > base ? b : base;
-            const long long q1 = e < base + cnt ? e : base + cnt;
-            for (long long q = q0; q < q1; ++q)
-                acc = fma(sm.v[q - base], w(sm.j[q - base]), acc);
-        }
-        __syncthreads();
+    for (; q + 8 <= e; q += 8) {
+        int j[8];
+        double v[8], x[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) j[i] = __ldg(a.ja + q + i);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) v[i] = __ldg(a.values + q + i);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) x[i] = w(j[i]);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) acc = fma(v[i], x[i], acc);
     }
-    return boundary ? w(static_cast<int>(s)) : acc;
+    for (; q < e; ++q) acc = fma(__ldg(a.values + q), w(__ldg(a.ja + q)), acc);
+    return acc;
 }
 
 // Sums NV values over the block; the totals end up in every lane of warp 0.
@@ -213,14 +191,12 @@ __global__ void flag_kernel(int n, int nb, const int* __restrict__ bnd, unsigned
 
 // r = f - A u, rh = r, p = v = 0; rho = (r, r), ff = (f, f).
 __global__ void __launch_bounds__(kThreads, kBlocksPerSm) init_kernel(Args a, double tol, int maxit) {
-    __shared__ Stage sm;
     double acc[2] = {0.0, 0.0};
     const long long stride = static_cast<long long>(gridDim.x) * kThreads;
     const double* u = a.u;
-    for (long long r0 = static_cast<long long>(blockIdx.x) * kThreads; r0 < a.n; r0 += stride) {
-        const double au = apply_tile(a, r0, sm, [u](int j) { return u[j]; });
-        const long long s = r0 + threadIdx.x;
-        if (s >= a.n) continue;
+    for (long long s = static_cast<long long>(blockIdx.x) * kThreads + threadIdx.x; s < a.n;
+         s += stride) {
+        const double au = apply_row(a, s, [u](int j) { return u[j]; });
         const double fs = a.f[s];
         const double r = fs - au;
         a.r[s] = r;
@@ -270,14 +246,12 @@ __global__ void __launch_bounds__(kThreads, kBlocksPerSm) p_kernel(Args a) {
 __global__ void __launch_bounds__(kThreads, kBlocksPerSm) spmv_v_kernel(Args a) {
     State* st = a.st;
     if (st->done) return;
-    __shared__ Stage sm;
     double acc[1] = {0.0};
     const long long stride = static_cast<long long>(gridDim.x) * kThreads;
     const double* p = a.p;
-    for (long long r0 = static_cast<long long>(blockIdx.x) * kThreads; r0 < a.n; r0 += stride) {
-        const double v = apply_tile(a, r0, sm, [p](int j) { return __ldg(p + j); });
-        const long long s = r0 + threadIdx.x;
-        if (s >= a.n) continue;
+    for (long long s = static_cast<long long>(blockIdx.x) * kThreads + threadIdx.x; s < a.n;
+         s += stride) {
+        const double v = apply_row(a, s, [p](int j) { return __ldg(p + j); });
         a.v[s] = v;
         acc[0] = fma(a.rh[s], v, acc[0]);
     }
@@ -303,14 +277,12 @@ __global__ void __launch_bounds__(kThreads, kBlocksPerSm) s_kernel(Args a) {
 __global__ void __launch_bounds__(kThreads, kBlocksPerSm) spmv_t_kernel(Args a) {
     State* st = a.st;
     if (st->done) return;
-    __shared__ Stage sm;
     double acc[3] = {0.0, 0.0, 0.0};
     const long long stride = static_cast<long long>(gridDim.x) * kThreads;
     const double* sv = a.s;
-    for (long long r0 = static_cast<long long>(blockIdx.x) * kThreads; r0 < a.n; r0 += stride) {
-        const double ti = apply_tile(a, r0, sm, [sv](int j) { return __ldg(sv + j); });
-        const long long i = r0 + threadIdx.x;
-        if (i >= a.n) continue;
+    for (long long i = static_cast<long long>(blockIdx.x) * kThreads + threadIdx.x; i < a.n;
+         i += stride) {
+        const double ti = apply_row(a, i, [sv](int j) { return __ldg(sv + j); });
         const double si = sv[i];
         a.t[i] = ti;
         acc[0] = fma(ti, si, acc[0]);
