@@ -12,11 +12,12 @@
 //           u = u + alpha p + omega s;     r = s - omega t
 //           stop when (r, r) <= tol^2 (f, f); beta = ((rh, r) / rho) (alpha / omega)
 //
-// On this part the iteration is HBM-bound: each step reads the operator
-// (12 B per stored weight, twice) and a handful of vectors; the operator
-// passes are bound by their gathers, each thread summing its own row in row
-// order with eight gathers in flight. It is laid out as five kernels per
-// iteration, each one pass over the rows:
+// The iteration streams memory, so HBM bandwidth is its roofline: each step
+// reads the operator (12 B per stored weight, twice) and a handful of
+// vectors. What holds the operator passes below it is the latency of their
+// gathers (one per stored weight), which each thread hides by summing its
+// own row in row order with eight gathers in flight. It is laid out as five
+// kernels per iteration, each one pass over the rows:
 //   p_kernel       p = r + beta (p - omega v)
 //   spmv_v_kernel  v = A p, with the partial sums of (rh, v)
 //   s_kernel       s = r - alpha v
