@@ -20,6 +20,14 @@ def test_algorithmic_counts():
     assert bench.HBM_COMPULSORY_PER_STENCIL == (4 + 24) * 35 + 20 == 1000
 
 
+def test_solve_byte_model():
+    # one BiCGSTAB iteration: two operator passes (12 B per weight; row
+    # pointer, flag, output and one gather per row) and the vector passes
+    from rbf_b200 import run
+    assert run.solve_bytes(1, 0) == 2 * (4 + 1 + 8) + 8 + 8 + 8 + 24 + 32 + 56 == 162
+    assert run.solve_bytes(4194304, 117672830) == 24 * 117672830 + 162 * 4194304
+
+
 def test_traffic_from_the_committed_profile():
     t = bench.traffic_per_launch("fp64")
     assert t is not None and 0.3e9 < t < 2e9  # DRAM bytes per full-size launch
