@@ -116,3 +116,37 @@ def test_grid_and_identity_operator():
                                     ia=np.zeros(n + 1, np.int32), bnd=np.arange(n, dtype=np.int32),
                                     tol=0.0, maxit=1, grid=O.solve_grid(n, 148))
         assert st == 0 and it == 1 and rel == 0.0 and np.array_equal(u, f)
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_random_stencil_operators(seed):
+    """Random diagonally dominant operators with stencil rows (self first),
+    fixed-width or ragged, some rows identity: the oracle's iterate solves
+    the dense system."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(50, 400))
+    ragged = seed % 2 == 1
+    kv = rng.integers(3, 12, size=n) if ragged else np.full(n, 7)
+    ia = np.zeros(n + 1, np.int64)
+    ia[1:] = np.cumsum(kv)
+    ja = np.empty(ia[-1], np.int32)
+    vals = np.empty(ia[-1])
+    A = np.zeros((n, n))
+    for s in range(n):
+        others = rng.choice(np.delete(np.arange(n), s), size=kv[s] - 1, replace=False)
+        cols = np.concatenate([[s], others])
+        w = rng.uniform(-1.0, 1.0, size=kv[s])
+        w[0] = np.abs(w[1:]).sum() + rng.uniform(0.5, 2.0)
+        ja[ia[s]:ia[s + 1]] = cols
+        vals[ia[s]:ia[s + 1]] = w
+        A[s, cols] = w
+    bnd = np.sort(rng.choice(n, size=n // 10, replace=False)).astype(np.int32)
+    A[bnd] = 0.0
+    A[bnd, bnd] = 1.0
+    f = rng.standard_normal(n)
+    kw = dict(ia=ia.astype(np.int32)) if ragged else dict(k=7)
+    st, u, it, rel = O.bicgstab(vals, ja, f, np.zeros(n), bnd=bnd, tol=1e-13, maxit=2000,
+                                grid=O.solve_grid(n, 148), **kw)
+    assert st == 0 and rel <= 1e-13
+    ud = np.linalg.solve(A, f)
+    assert np.abs(u - ud).max() <= 1e-10 * np.abs(ud).max()
