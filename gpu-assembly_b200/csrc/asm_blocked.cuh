@@ -1,0 +1,526 @@
+// asm_blocked.cuh -- batched RBF-FD assembly on sm_100a with the saddle-point
+// system held in shared memory and factored by a blocked right-looking
+// Gaussian elimination with row-implicit partial pivoting.
+//
+// Replaces assemble_interp_weights<Config> (src/rbf_operators.h:292-376),
+// whose solve is cuSolverDx gesv_partial_pivot with one stencil per CTA.
+//
+// One warp owns one stencil; a CTA holds BLOCK / 32 warps and the grid is
+// persistent. The system is not padded: n = npoly(P) + k_s unknowns for the
+// stencil's own k_s, any n <= NMAX. It is stored row-major in S (row =
+// equation, column = unknown) with the NRHS right-hand sides as columns
+// n .. n+NRHS-1, polynomial block first: equations [P^T rows (NP), node rows
+// (k_s)], unknowns [lambda (NP), w (k_s)]. Rows are never swapped: piv[c] is
+// the row that became the pivot row at step c, alive[r] is cleared then.
+//
+// The elimination runs in panels of PB columns. For panel [c0, c0+PB):
+//   1. the rows not yet pivoted are listed in ascending order (act[]); lane
+//      l takes list positions l, l+32, ... and loads their PB panel columns
+//      into registers;
+//   2. PB steps on the panel columns only. Step c: pivot = the unused row of
+//      largest key (a 32-bit key: the magnitude word of a(r,c) without its 7
+//      lowest bits, plus one, with 127 - list position in those bits, so ties
+//      go to the lowest row -- the oracle's rule), found by one warp
+//      reduction whose operands were formed at the end of the previous step;
+//      the pivot row's owner writes its whole panel row to S (final: L
+//      multipliers left of c, the pivot, U right of it) and 1 / pivot (rounded
+//      once, the oracle's reciprocal); every other unused row takes
+//      l = a(r,c) * (1 / pivot) and a(r,j) = fma(-l, u(j), a(r,j)) for the
+//      panel columns j > c;
+//   3. rows still unused write their panel columns (now the L multipliers)
+//      back to S;
+//   4. the panel's pivot rows over the trailing columns (right-hand sides
+//      included): row p_t takes the updates of steps t' < t, in order;
+//   5. every unused row over the trailing columns: the PB updates of the
+//      panel, in order, multipliers from registers, pivot-row values read
+//      once per column pair and broadcast to the warp.
+// Every matrix and right-hand-side element receives exactly the fused
+// multiply-adds of the unblocked elimination, in the same order, so the FP64
+// result is bit-identical to the oracle's.
+//
+// Back substitution is column oriented, as the oracle's: lane l holds the
+// transformed right-hand sides of the rows pivoted at steps l, l+32, ...;
+// for c = n-1 .. 0 the owner of step c forms x_c = y * (1 / pivot_c) and
+// broadcasts it by shuffle, and the rows pivoted before c update with
+// u(row, c).
+#pragma once
+
+#include <cstdint>
+
+#include "asm_kernel.cuh"
+
+namespace rbfb {
+
+template <typename T, int NMAX, int NRHS, int P, int Q, bool MIXED, int PB>
+struct BlkCfg {
+    static constexpr int G = 32;  // lanes per stencil: one warp
+    static constexpr int NP = npoly(P);
+    static constexpr int KMAX = NMAX - NP;
+    static constexpr int R = (NMAX + G - 1) / G;  // list positions per lane
+    static constexpr int VE = 16 / (int)sizeof(T);  // elements per 16-byte vector
+    static_assert(!MIXED, "the blocked kernel is FP64");
+    static_assert(PB % VE == 0, "panels are whole vectors");
+    static_assert(NMAX <= 128, "pivot keys carry the list position in 7 bits");
+    static constexpr int WMAX = NMAX + NRHS;  // columns: unknowns + right-hand sides
+    // Row stride in vectors: odd, so the 32 rows a warp reads down one column
+    // fall in different bank groups (4 wavefronts for 32 vectors).
+    static constexpr int LV0 = (WMAX + VE - 1) / VE;
+    static constexpr int LDSV = (LV0 % 2) ? LV0 : LV0 + 1;
+    static constexpr int LDS = LDSV * VE;
+    static constexpr int al16(int b) { return (b + 15) & ~15; }
+    static constexpr int off_cx = 0;
+    static constexpr int off_cy = off_cx + al16(8 * KMAX);
+    static constexpr int off_s = off_cy + al16(8 * KMAX);
+    static constexpr int off_x = off_s + al16(NMAX * LDS * (int)sizeof(T));
+    static constexpr int off_pinv = off_x + al16(NMAX * NRHS * (int)sizeof(T));
+    static constexpr int off_piv = off_pinv + al16(NMAX * (int)sizeof(T));
+    static constexpr int off_act = off_piv + al16(4 * NMAX);
+    static constexpr int off_alive = off_act + al16(4 * NMAX);
+    // next stencil, prefetched while this one is solved: its ja row, its
+    // centre (x, y) and its CSR bounds ia[s], ia[s + 1] (+ size, next item)
+    static constexpr int off_nja = off_alive + al16(NMAX);
+    static constexpr int off_nxy = off_nja + al16(4 * KMAX);
+    static constexpr int off_nia = off_nxy + 16;
+    static constexpr int bytes = off_nia + 16;
+};
+
+// 16-byte vector moves between shared memory and register arrays.
+__device__ __forceinline__ void ldv(const double* s, double* d) {
+    const double2 v = *reinterpret_cast<const double2*>(s);
+    d[0] = v.x;
+    d[1] = v.y;
+}
+__device__ __forceinline__ void ldv(const float* s, float* d) {
+    const float4 v = *reinterpret_cast<const float4*>(s);
+    d[0] = v.x;
+    d[1] = v.y;
+    d[2] = v.z;
+    d[3] = v.w;
+}
+__device__ __forceinline__ void stv(double* s, const double* d) {
+    *reinterpret_cast<double2*>(s) = make_double2(d[0], d[1]);
+}
+__device__ __forceinline__ void stv(float* s, const float* d) {
+    *reinterpret_cast<float4*>(s) = make_float4(d[0], d[1], d[2], d[3]);
+}
+
+// The word a pivot key is made from: the high 32 bits of a binary64 value
+// (sign, exponent, 20 leading mantissa bits), all 32 bits of a binary32 one.
+__device__ __forceinline__ uint32_t hiword(double v) {
+    return (uint32_t)((unsigned long long)__double_as_longlong(v) >> 32);
+}
+__device__ __forceinline__ uint32_t hiword(float v) { return __float_as_uint(v); }
+
+template <typename T, int NMAX, int NRHS, int P, int Q, bool MIXED, int PB, bool PF>
+__device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, char* smem,
+                                             int lane) {
+    using C = BlkCfg<T, NMAX, NRHS, P, Q, MIXED, PB>;
+    constexpr int G = C::G, NP = C::NP, R = C::R, VE = C::VE, LDS = C::LDS;
+    constexpr unsigned FULL = 0xffffffffu;
+    double* cx = reinterpret_cast<double*>(smem + C::off_cx);
+    double* cy = reinterpret_cast<double*>(smem + C::off_cy);
+    T* S = reinterpret_cast<T*>(smem + C::off_s);
+    T* X = reinterpret_cast<T*>(smem + C::off_x);
+    T* pinv = reinterpret_cast<T*>(smem + C::off_pinv);
+    int* piv = reinterpret_cast<int*>(smem + C::off_piv);
+    int* act = reinterpret_cast<int*>(smem + C::off_act);
+    unsigned char* alive = reinterpret_cast<unsigned char*>(smem + C::off_alive);
+    int* nja = reinterpret_cast<int*>(smem + C::off_nja);
+    double* nxy = reinterpret_cast<double*>(smem + C::off_nxy);
+    int* nia = reinterpret_cast<int*>(smem + C::off_nia);
+
+    // With PF, stencil s was prefetched (by the previous call of this warp, or
+    // by prefetch_first): its neighbour coordinates wait in cx/cy (raw), its
+    // centre in nxy, its CSR bounds in nia. Without PF everything comes from
+    // global memory.
+    int off, ks;
+    double x0, y0;
+    if constexpr (PF) {
+        cp_async_wait_all();
+        __syncwarp();
+        x0 = nxy[0];
+        y0 = nxy[1];
+        off = p.ia ? nia[0] : (s - p.row_base) * p.k;
+        ks = p.ia ? nia[1] - off : p.k;
+        __syncwarp();  // read before the slots are refilled below
+    } else {
+        x0 = p.x[s];
+        y0 = p.y[s];
+        off = p.ia ? p.ia[s] : (s - p.row_base) * p.k;
+        ks = p.ia ? p.ia[s + 1] - off : p.k;
+    }
+    const int n = NP + ks;
+    const int W = n + NRHS;  // columns in use
+    if (PF && sn >= 0 && lane == 0) {  // prefetch stage 1: next centre and CSR bounds
+        cp_async8(nxy, p.x + sn);
+        cp_async8(nxy + 1, p.y + sn);
+        if (p.ia) {
+            cp_async4(nia, p.ia + sn);
+            cp_async4(nia + 1, p.ia + sn + 1);
+        }
+    }
+
+    // ---- gather + FP64 shift (+ minimum image), src/rbf_operators.h:354-358,
+    // and the power-of-two radius scale
+    int e;
+    {
+        constexpr int KPL = (C::KMAX + G - 1) / G;
+        double gx[KPL], gy[KPL];
+        int emax = -100000;
+#pragma unroll
+        for (int t = 0; t < KPL; ++t) {
+            const int j = lane + t * G;
+            gx[t] = 0.0;
+            gy[t] = 0.0;
+            if (j < ks) {
+                double xn, yn;
+                if constexpr (PF) {
+                    xn = cx[j];
+                    yn = cy[j];
+                } else {
+                    const int nb = __ldg(p.ja + off + j);
+                    xn = __ldg(p.x + nb);
+                    yn = __ldg(p.y + nb);
+                }
+                gx[t] = min_image(dsub(xn, x0), p.Lx);
+                gy[t] = min_image(dsub(yn, y0), p.Ly);
+                if (gx[t] != 0.0) emax = max(emax, ilogb(fabs(gx[t])) + 1);
+                if (gy[t] != 0.0) emax = max(emax, ilogb(fabs(gy[t])) + 1);
+            }
+        }
+        e = __reduce_max_sync(FULL, emax);
+        e = (p.scale && e > -100000) ? e : 0;
+#pragma unroll
+        for (int t = 0; t < KPL; ++t) {
+            const int j = lane + t * G;
+            if (j < ks) {
+                cx[j] = scalbn(gx[t], -e);
+                cy[j] = scalbn(gy[t], -e);
+            }
+        }
+    }
+    __syncwarp();
+
+    // ---- fill S: phi block (each unordered pair once, a flat walk over the
+    // lanes), monomial rows and columns, zero polynomial block, right-hand
+    // sides (fill_matrix / fill_rhs, src/rbf_operators.h:116-185)
+    {
+        const int npair = ks * (ks - 1) / 2;
+        int i = 0, j = 1 + lane;
+        while (i < ks - 1 && j >= ks) {
+            j += i + 2 - ks;
+            ++i;
+        }
+        for (int t = lane; t < npair; t += G) {
+            const T v = static_cast<T>(phs64<Q>(dist2(dsub(cx[j], cx[i]), dsub(cy[j], cy[i]))));
+            S[(NP + i) * LDS + NP + j] = v;
+            S[(NP + j) * LDS + NP + i] = v;
+            j += G;
+            while (i < ks - 1 && j >= ks) {
+                j += i + 2 - ks;
+                ++i;
+            }
+        }
+    }
+    for (int i = lane; i < ks; i += G) {
+        const int r = NP + i;
+        T* Sr = S + r * LDS;
+        const double xi = cx[i], yi = cy[i];
+        double mon[NP];
+        monomials<P>(xi, yi, mon);
+#pragma unroll
+        for (int m = 0; m < NP; ++m) {
+            Sr[m] = static_cast<T>(mon[m]);
+            S[m * LDS + r] = static_cast<T>(mon[m]);
+        }
+        Sr[r] = T(0);
+        double rv[NRHS];
+        rhs_node<P, Q, NRHS>(p, xi, yi, e, rv);
+#pragma unroll
+        for (int q = 0; q < NRHS; ++q) Sr[n + q] = static_cast<T>(rv[q]);
+    }
+    for (int f = lane; f < NP * NP; f += G) S[(f / NP) * LDS + f % NP] = T(0);
+    for (int r = lane; r < NP; r += G) {
+#pragma unroll
+        for (int q = 0; q < NRHS; ++q)
+            S[r * LDS + n + q] = static_cast<T>(q < p.nrhs ? rhs_poly<P>(p, q, r, e) : 0.0);
+    }
+    for (int r = lane; r < NMAX; r += G) alive[r] = r < n ? 1 : 0;
+
+    // prefetch stage 2: the next stencil's ja row (its bounds have landed)
+    if constexpr (PF) {
+        int offn = 0, ksn = 0;
+        if (sn >= 0) {
+            if (p.ia) {
+                cp_async_wait_all();
+                __syncwarp();
+                offn = nia[0];
+                ksn = nia[1] - offn;
+            } else {
+                offn = (sn - p.row_base) * p.k;
+                ksn = p.k;
+            }
+            for (int j = lane; j < ksn; j += G) cp_async4(nja + j, p.ja + offn + j);
+        }
+        __syncwarp();
+        if (lane == 0) nia[2] = ksn;
+    }
+    __syncwarp();
+
+    // ---- blocked elimination
+    int info = 0;
+#pragma unroll 1
+    for (int c0 = 0; c0 < n; c0 += PB) {
+        // 1. the unused rows, ascending, and this lane's panel rows
+        int m = 0;
+#pragma unroll
+        for (int j = 0; j < R; ++j) {
+            const int r = lane + G * j;
+            const bool a = r < NMAX && alive[r];
+            const unsigned b = __ballot_sync(FULL, a);
+            if (a) act[m + __popc(b & ((1u << lane) - 1u))] = r;
+            m += __popc(b);
+        }
+        __syncwarp();
+        T a[R][PB];
+        int arow[R];
+        uint32_t kmask[R], kcon[R];
+#pragma unroll
+        for (int sl = 0; sl < R; ++sl) {
+            const int pos = lane + G * sl;
+            const bool v = pos < m;
+            arow[sl] = v ? act[pos] : 0;
+            kmask[sl] = v ? 0x7fffff80u : 0u;
+            kcon[sl] = v ? 255u - (uint32_t)pos : 0u;
+            const T* src = S + arow[sl] * LDS + c0;
+#pragma unroll
+            for (int v4 = 0; v4 < PB; v4 += VE) ldv(src + v4, &a[sl][v4]);
+        }
+        const int tend = min(PB, n - c0);  // steps in this panel
+        // look-ahead operands of the pivot search of the panel's first column
+        uint32_t pkey;
+        T pinvl;
+        auto keys = [&](int t) {
+            uint32_t best = 0;
+            T bv = T(1);
+#pragma unroll
+            for (int sl = 0; sl < R; ++sl) {
+                const uint32_t kk = (hiword(a[sl][t]) & kmask[sl]) + kcon[sl];
+                if (kk > best) {
+                    best = kk;
+                    bv = a[sl][t];
+                }
+            }
+            pkey = best;
+            pinvl = recip_rn(bv);  // the oracle's 1 / pivot, if this lane owns the pivot
+        };
+        keys(0);
+        // 2. the panel's steps
+#pragma unroll
+        for (int t = 0; t < PB; ++t) {
+            if (t < tend) {
+                const int c = c0 + t;
+                const uint32_t mk = __reduce_max_sync(FULL, pkey);
+                if (mk < 256u && info == 0) info = c + 1;  // zero pivot column
+                const int pos = 127 - (int)(mk & 127u);
+                const int owner = pos & (G - 1), osl = pos / G;
+                if (lane == owner) {
+#pragma unroll
+                    for (int sl = 0; sl < R; ++sl) {
+                        if (sl == osl) {
+                            T* dst = S + arow[sl] * LDS + c0;
+#pragma unroll
+                            for (int v4 = 0; v4 < PB; v4 += VE) stv(dst + v4, &a[sl][v4]);
+                            piv[c] = arow[sl];
+                            alive[arow[sl]] = 0;
+                            kmask[sl] = 0u;
+                            kcon[sl] = 0u;
+                        }
+                    }
+                    pinv[c] = pinvl;
+                }
+                __syncwarp();
+                const T inv = pinv[c];
+                const T* U = S + piv[c] * LDS + c0;
+                // multipliers of the unused rows (0 for the others)
+                T l[R];
+#pragma unroll
+                for (int sl = 0; sl < R; ++sl) {
+                    l[sl] = kmask[sl] ? a[sl][t] * inv : T(0);
+                    a[sl][t] = l[sl];
+                }
+                // the panel columns right of c
+                if (t + 1 < PB) {
+                    T u[PB];
+#pragma unroll
+                    for (int v4 = ((t + 1) / VE) * VE; v4 < PB; v4 += VE) ldv(U + v4, &u[v4]);
+#pragma unroll
+                    for (int j = t + 1; j < PB; ++j)
+#pragma unroll
+                        for (int sl = 0; sl < R; ++sl) a[sl][j] = fma(-l[sl], u[j], a[sl][j]);
+                    if (t + 1 < tend) keys(t + 1);
+                }
+            }
+        }
+        // 3. rows still unused: their L multipliers back to S
+#pragma unroll
+        for (int sl = 0; sl < R; ++sl) {
+            if (kmask[sl]) {
+                T* dst = S + arow[sl] * LDS + c0;
+#pragma unroll
+                for (int v4 = 0; v4 < PB; v4 += VE) stv(dst + v4, &a[sl][v4]);
+            }
+        }
+        __syncwarp();
+        const int jt = c0 + PB;  // first trailing column
+        if (jt >= W) break;
+        const int nv = (W - jt + VE - 1) / VE;  // trailing column vectors
+        int prw[PB];
+#pragma unroll
+        for (int t = 0; t < PB; ++t) prw[t] = piv[c0 + (t < tend ? t : 0)];
+        // 4. the panel's pivot rows over the trailing columns
+        for (int v = lane; v < nv; v += G) {
+            const int col = jt + v * VE;
+            T u[PB][VE];
+#pragma unroll
+            for (int t = 0; t < PB; ++t) {
+                if (t < tend) {
+                    ldv(S + prw[t] * LDS + col, u[t]);
+#pragma unroll
+                    for (int tp = 0; tp < t; ++tp) {
+                        const T lv = S[prw[t] * LDS + c0 + tp];
+#pragma unroll
+                        for (int q = 0; q < VE; ++q) u[t][q] = fma(-lv, u[tp][q], u[t][q]);
+                    }
+                    stv(S + prw[t] * LDS + col, u[t]);
+                }
+            }
+        }
+        __syncwarp();
+        // 5. the unused rows over the trailing columns (all lanes walk the same
+        // columns: the pivot-row values are broadcast loads)
+        if (tend == PB) {
+            bool any[R];
+#pragma unroll
+            for (int sl = 0; sl < R; ++sl) any[sl] = __any_sync(FULL, kmask[sl] != 0u);
+#pragma unroll 1
+            for (int v = 0; v < nv; ++v) {
+                const int col = jt + v * VE;
+                T u[PB][VE];
+#pragma unroll
+                for (int t = 0; t < PB; ++t) ldv(S + prw[t] * LDS + col, u[t]);
+#pragma unroll
+                for (int sl = 0; sl < R; ++sl) {
+                    if (any[sl]) {
+                        T* cp = S + arow[sl] * LDS + col;
+                        T cv[VE];
+                        ldv(cp, cv);
+#pragma unroll
+                        for (int t = 0; t < PB; ++t)
+#pragma unroll
+                            for (int q = 0; q < VE; ++q) cv[q] = fma(-a[sl][t], u[t][q], cv[q]);
+                        if (kmask[sl]) stv(cp, cv);
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    }
+
+    // ---- back substitution (column oriented): lane l holds the transformed
+    // right-hand sides of the rows pivoted at steps l, l + 32, ...
+    T y[R][NRHS];
+    int prow_t[R];
+#pragma unroll
+    for (int sl = 0; sl < R; ++sl) {
+        const int t = lane + G * sl;
+        prow_t[sl] = t < n ? piv[t] : 0;
+#pragma unroll
+        for (int q = 0; q < NRHS; ++q) y[sl][q] = t < n ? S[prow_t[sl] * LDS + n + q] : T(0);
+    }
+    // prefetch stage 3: the next stencil's neighbour coordinates into cx/cy
+    if (const int ksn = PF ? nia[2] : 0; ksn > 0) {
+        cp_async_wait_all();
+        for (int j = lane; j < ksn; j += G) {
+            const int nb = nja[j];
+            cp_async8(cx + j, p.x + nb);
+            cp_async8(cy + j, p.y + nb);
+        }
+    }
+#pragma unroll 1
+    for (int c = n - 1; c >= 0; --c) {
+        const int owner = c & (G - 1), osl = c / G;
+        const T dv = pinv[c];
+        T xq[NRHS];
+#pragma unroll
+        for (int q = 0; q < NRHS; ++q) {
+            T v = y[0][q];
+#pragma unroll
+            for (int sl = 1; sl < R; ++sl) v = (osl == sl) ? y[sl][q] : v;
+            xq[q] = __shfl_sync(FULL, v * dv, owner);
+        }
+        if (lane == 0) {
+#pragma unroll
+            for (int q = 0; q < NRHS; ++q) X[c * NRHS + q] = xq[q];
+        }
+#pragma unroll
+        for (int sl = 0; sl < R; ++sl) {
+            const int t = lane + G * sl;
+            const T u = (t < c) ? S[prow_t[sl] * LDS + c] : T(0);
+#pragma unroll
+            for (int q = 0; q < NRHS; ++q) y[sl][q] = fma(-u, xq[q], y[sl][q]);
+        }
+    }
+    __syncwarp();
+
+    // ---- scatter, src/rbf_operators.h:368-375
+    const bool bad = info != 0;
+    for (int q = 0; q < p.nrhs; ++q) {
+        double* dst = p.values[q] + off;
+        const int sh = -op_order(p.col_op[q]) * e;
+        for (int j = lane; j < ks; j += G) {
+            const double v = static_cast<double>(X[(NP + j) * NRHS + q]);
+            dst[j] = bad ? __longlong_as_double(0x7ff8000000000000ll) : scalbn(v, sh);
+        }
+    }
+    if (lane == 0 && p.info) p.info[s - p.row_base] = info;
+    __syncwarp();
+}
+
+template <typename T, int NMAX, int NRHS, int P, int Q, bool MIXED, int BLOCK, int MINB, int PB,
+          bool PF>
+__global__ void __launch_bounds__(BLOCK, MINB) blk_kernel(AsmParams p) {
+    using C = BlkCfg<T, NMAX, NRHS, P, Q, MIXED, PB>;
+    constexpr int G = C::G;
+    constexpr int GPB = BLOCK / G;  // warps (stencils in flight) per CTA
+    extern __shared__ __align__(16) char smem_raw[];
+    const int gib = threadIdx.x / G;
+    const int lane = threadIdx.x % G;
+    char* smem = smem_raw + gib * C::bytes;
+    const int n = p.nitems_dev ? *p.nitems_dev : p.nitems;
+    const int* list = (p.list && p.list_off_dev) ? p.list + *p.list_off_dev : p.list;
+    const int ngroups = gridDim.x * GPB;
+    auto claim = [&](int next_static) {
+        if (!p.work) return next_static;
+        int v = 0;
+        if (lane == 0) v = atomicAdd(p.work, 1);
+        return __shfl_sync(0xffffffffu, v, 0);
+    };
+    auto item = [&](int i) { return i < n ? (list ? list[i] : p.item_base + i) : -1; };
+    // One call site: the stencil body is inlined once. With PF each call
+    // also prefetches the next item's data (claimed one ahead).
+    int* next_it = reinterpret_cast<int*>(smem + C::off_nia) + 3;
+    int it = claim(blockIdx.x * GPB + gib);
+    if constexpr (PF) {
+        if (it < n) prefetch_first<C>(p, item(it), smem, lane, 0xffffffffu);
+    }
+    while (it < n) {
+        const int itn = claim(it + ngroups);
+        if (lane == 0) *next_it = itn;
+        assemble_blk<T, NMAX, NRHS, P, Q, MIXED, PB, PF>(p, item(it), PF ? item(itn) : -1, smem, lane);
+        it = *next_it;
+        __syncwarp();
+    }
+}
+
+}  // namespace rbfb

@@ -11,6 +11,10 @@
 //   PF       prefetch the next stencil's neighbour data (cp.async) while the
 //            current one is solved; off where the extra live state costs the
 //            register-bound elimination more than the gather latency it hides
+//
+// RBFB_BLK_VARIANT(name, T, NMAX, NRHS, P, Q, MIXED, BLOCK, MINB, PB, PF): the
+// blocked shared-memory kernel (asm_blocked.cuh), one warp per stencil, any
+// system size n <= NMAX, panels of PB columns.
 // The build compiles each line as its own translation unit.
 RBFB_VARIANT(f64_p2q3_n32_g16x2, double, 16, 2, 32, 3, 2, 3, false, 64, 6, false, true)
 RBFB_VARIANT(f64_p2q3_n32_g16x1, double, 16, 1, 32, 3, 2, 3, false, 64, 1, false, true)
@@ -23,3 +27,5 @@ RBFB_VARIANT(f64_p4q7_n64_smem, double, 16, 2, 64, 3, 4, 7, false, 32, 1, true, 
 RBFB_VARIANT(f64_p4q7_n80_smem, double, 16, 2, 80, 3, 4, 7, false, 32, 1, true, true)
 RBFB_VARIANT(mix_p4q7_n64_smem, float, 16, 2, 64, 3, 4, 7, true, 32, 1, true, true)
 RBFB_VARIANT(mix_p4q7_n80_smem, float, 16, 2, 80, 3, 4, 7, true, 32, 1, true, true)
+RBFB_BLK_VARIANT(b64_p3q5_n48_pb8, double, 48, 3, 3, 5, false, 96, 1, 8, true)
+RBFB_BLK_VARIANT(b64_p3q5_n48_pb8w1, double, 48, 3, 3, 5, false, 32, 1, 8, true)

@@ -4,6 +4,7 @@
 
 #include <cuda_runtime.h>
 
+#include "asm_blocked.cuh"
 #include "asm_kernel.cuh"
 #include "asm_variants.h"
 
@@ -32,7 +33,36 @@ Variant make_variant(const char* name) {
     return v;
 }
 
+template <typename T, int NMAX, int NRHS, int P, int Q, bool MIXED, int BLOCK, int MINB, int PB,
+          bool PF>
+Variant make_blk_variant(const char* name) {
+    using C = BlkCfg<T, NMAX, NRHS, P, Q, MIXED, PB>;
+    Variant v{};
+    v.name = name;
+    v.kernel = reinterpret_cast<const void*>(&blk_kernel<T, NMAX, NRHS, P, Q, MIXED, BLOCK, MINB, PB, PF>);
+    v.launch = [](dim3 grid, int block, size_t smem, cudaStream_t st, const AsmParams& p) {
+        blk_kernel<T, NMAX, NRHS, P, Q, MIXED, BLOCK, MINB, PB, PF><<<grid, block, smem, st>>>(p);
+    };
+    v.mixed = MIXED;
+    v.P = P;
+    v.Q = Q;
+    v.ntp = NMAX;
+    v.nrhs = NRHS;
+    v.group = C::G;
+    v.block = BLOCK;
+    v.smem_group = C::bytes;
+    v.smem_block = C::bytes * (BLOCK / C::G);
+    return v;
+}
+
 }  // namespace rbfb
+
+#define RBFB_DEFINE_BLK_VARIANT(name, T, NMAX, NRHS, P, Q, MIXED, BLOCK, MINB, PB, PF)          \
+    namespace rbfb {                                                                           \
+    Variant variant_##name() {                                                                 \
+        return make_blk_variant<T, NMAX, NRHS, P, Q, MIXED, BLOCK, MINB, PB, PF>(#name);       \
+    }                                                                                          \
+    }
 
 #define RBFB_DEFINE_VARIANT(name, T, GR, GC, NTP, NRHS, P, Q, MIXED, BLOCK, MINB, SMEM, PF)    \
     namespace rbfb {                                                                           \

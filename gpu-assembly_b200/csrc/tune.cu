@@ -21,6 +21,30 @@ const char* rbfb_variant_name(int index) {
     return (index >= 0 && index < static_cast<int>(vs.size())) ? vs[index].name : nullptr;
 }
 
+int rbfb_select_variant(rbfb_ctx* ctx, const rbfb_desc* desc, int k, int index,
+                        int blocks_per_sm) {
+    if (!ctx) return RBFB_EINVAL;
+    int rc = check_desc(ctx, desc);
+    if (rc) return rc;
+    const auto& vs = variants();
+    if (index < 0 || index >= static_cast<int>(vs.size()) || k < 1 || blocks_per_sm < 0)
+        return fail(ctx, RBFB_EINVAL, "bad variant index, k or blocks_per_sm");
+    const int P = desc->degree;
+    const int Q = desc->phs ? desc->phs : 2 * P - 1;
+    const int n = k + npoly(P);
+    const bool mixed = desc->precision == RBFB_FP32_IR;
+    int ntp = 1 << 30;
+    for (const auto& v : vs)
+        if (v.mixed == mixed && v.P == P && v.Q == Q && v.ntp >= n) ntp = std::min(ntp, v.ntp);
+    const auto& v = vs[index];
+    if (v.mixed != mixed || v.P != P || v.Q != Q || v.ntp != ntp)
+        return fail(ctx, RBFB_EINVAL, std::string("shape ") + v.name +
+                                          " does not serve this precision, degree, PHS and size");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->tuned[std::make_tuple(mixed ? 1 : 0, P, Q, ntp)] = LaunchShape{index, blocks_per_sm};
+    return RBFB_OK;
+}
+
 int rbfb_autotune(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const double* x,
                   const double* y, int k, const int* ja, double* const* values_h) {
     if (!ctx) return RBFB_EINVAL;

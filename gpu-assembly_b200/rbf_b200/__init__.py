@@ -112,6 +112,7 @@ _PROTOS = {
     "rbfb_solve_dp": (_i, [_vp, _vp, _vp, _vp, _vp]),
     "rbfb_autotune": (_i, [_vp, C.POINTER(Desc), _i, _vp, _vp, _i, _vp, _vp]),
     "rbfb_variant_name": (C.c_char_p, [_i]),
+    "rbfb_select_variant": (_i, [_vp, C.POINTER(Desc), _i, _i, _i]),
     "rbfb_server_create": (_i, [C.POINTER(_vp), _i, C.c_size_t, _i]),
     "rbfb_server_submit": (_i, [_vp, C.POINTER(Request), C.POINTER(_ll)]),
     "rbfb_server_poll": (_i, [_vp, _ll, _i, C.POINTER(Result)]),
@@ -330,6 +331,11 @@ class Context:
                                  _ptr(ja), tab)
         return self._check(st, "autotune")
 
+    def select_variant(self, desc: Desc, k, index, blocks_per_sm=0):
+        """Pin compiled shape `index` for desc's class of k-node stencils."""
+        st = lib().rbfb_select_variant(self.h, C.byref(desc), k, index, blocks_per_sm)
+        return self._check(st, "select_variant")
+
     # ---- node renumbering (permutations in gather form: perm[new] = old)
     def curve_keys(self, x, y, keys, ndiv=16, curve=MORTON, bbox=None, stream=None):
         """int64 device keys <- Morton (curve=MORTON) or Hilbert curve keys."""
@@ -370,6 +376,14 @@ def knn_stencils_static(x, y, k, ja, period=None, stream=None):
 def variant_name(index: int):
     v = lib().rbfb_variant_name(index)
     return None if v is None else v.decode()
+
+
+def variant_names():
+    """Names of every compiled kernel shape, by index."""
+    out = []
+    while (v := variant_name(len(out))) is not None:
+        out.append(v)
+    return out
 
 
 def renumber_stencils(n, k, ja, perm, inv, ja_out, stream=None):

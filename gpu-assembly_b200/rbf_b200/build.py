@@ -38,8 +38,9 @@ def nvcc() -> str:
 
 
 def _variant_lines():
+    """(macro suffix, arguments) of every shape line of asm_variant_list.h."""
     text = (CSRC / "asm_variant_list.h").read_text()
-    return re.findall(r"^RBFB_VARIANT\((.*)\)\s*$", text, flags=re.M)
+    return re.findall(r"^RBFB_(VARIANT|BLK_VARIANT)\((.*)\)\s*$", text, flags=re.M)
 
 
 def _sources():
@@ -49,11 +50,11 @@ def _sources():
     units = []
     for f in sorted(CSRC.glob("*.cu")):
         units.append((f, BUILD / (f.stem + ".o")))
-    for args in _variant_lines():
+    for kind, args in _variant_lines():
         name = args.split(",")[0].strip()
         src = gen / f"v_{name}.cu"
         body = ('#include "asm_variant_make.cuh"\n'
-                f"RBFB_DEFINE_VARIANT({args})\n")
+                f"RBFB_DEFINE_{kind}({args})\n")
         if not src.exists() or src.read_text() != body:
             src.write_text(body)
         units.append((src, BUILD / f"v_{name}.o"))

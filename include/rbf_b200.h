@@ -301,6 +301,14 @@ int rbfb_autotune(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const dou
  * "mix_p3q5_n48_g16x2", or NULL past the last one. */
 const char* rbfb_variant_name(int index);
 
+/* Pins compiled shape `index` (and CTAs per SM, 0 = the occupancy maximum)
+ * for the systems of desc's precision, degree and PHS exponent with k-node
+ * stencils, as rbfb_autotune would record it. RBFB_EINVAL when the shape
+ * does not serve that class. No reference counterpart (the reference fixes
+ * its kernel at compile time, src/rbf_operators.h:187-290). */
+int rbfb_select_variant(rbfb_ctx* ctx, const rbfb_desc* desc, int k, int index,
+                        int blocks_per_sm);
+
 /* ---- serving ---------------------------------------------------------------- */
 /* Continuous-batching assembly server: requests (node sets of any size) are
  * admitted as slots and HBM budget free up, their k-NN and assembly overlap

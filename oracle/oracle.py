@@ -7,7 +7,10 @@ product. It loads
 * ``oracle/_build/liboracle.so`` -- the CPU restatement of the reference's
   assembly path (``oracle/rbf_oracle.cpp``), and
 * ``oracle/_ref/libref_knn.so`` -- the reference's own nanoflann / ckdtree
-  stencil searches compiled from the reference sources (``oracle/Makefile``).
+  stencil searches compiled from the reference sources (``oracle/Makefile``),
+* ``oracle/_ref/libref_fill.so`` -- the reference's own ``fill_matrix`` /
+  ``fill_rhs`` templates (``src/rbf_operators.h:39-185``) compiled from its
+  header against a declarations-only cuSolverDx stand-in.
 """
 from __future__ import annotations
 
@@ -20,11 +23,13 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "_build" / "liboracle.so"
 REF_SO = HERE / "_ref" / "libref_knn.so"
+REF_FILL_SO = HERE / "_ref" / "libref_fill.so"
 
 OP_INTERP, OP_LAPLACE, OP_DX, OP_DY, OP_DXX, OP_DYY, OP_DXY = 1, 2, 4, 8, 16, 32, 64
 
 _lib = None
 _ref = None
+_ref_fill = None
 
 _dp = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
@@ -84,6 +89,10 @@ def lib():
         L.orc_renumber_stencils.argtypes = [C.c_int, C.c_int, _ip, _ip, _ip]
         L.orc_renumber_csr.restype = None
         L.orc_renumber_csr.argtypes = [C.c_int, _ip, _ip, _ip, _ip, _ip]
+        L.orc_system.restype = C.c_int
+        L.orc_system.argtypes = [C.c_int, _dp, _dp, C.c_int, _ip, C.c_int, C.c_int, C.c_int,
+                                 C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_double,
+                                 _dp, _dp, _dp]
         L.orc_phs.restype = C.c_double
         L.orc_phs.argtypes = [C.c_int, C.c_double]
         L.orc_set_threads.argtypes = [C.c_int]
@@ -106,6 +115,64 @@ def ref():
         L.ref_set_threads.argtypes = [C.c_int]
         _ref = L
     return _ref
+
+
+def ref_fill_lib():
+    """The reference's own fill templates, or None when not built here."""
+    global _ref_fill
+    if _ref_fill is None:
+        if not REF_FILL_SO.exists():
+            return None
+        L = C.CDLL(str(REF_FILL_SO))
+        L.ref_fill.restype = C.c_int
+        L.ref_fill.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, C.c_int, _dp, _dp, _dp, _dp]
+        _ref_fill = L
+    return _ref_fill
+
+
+def ref_fill(xs, ys, P, Q, xc=(), yc=()):
+    """The reference's fill_matrix and fill_rhs (src/rbf_operators.h:116-185)
+    on stencil-local coordinates: (M, B) as numpy (nt, nt) and (nt, nc)
+    arrays in the reference's layout (node rows first, then the monomials),
+    or None when the library or the (k, P, Q) combination is absent."""
+    L = ref_fill_lib()
+    if L is None:
+        return None
+    xs, ys = _f64(xs), _f64(ys)
+    xc, yc = _f64(np.asarray(xc, np.float64).ravel()), _f64(np.asarray(yc, np.float64).ravel())
+    k = xs.size
+    nt = k + npoly(P)
+    M = np.zeros(nt * nt)
+    B = np.zeros(nt * max(xc.size, 1))
+    if L.ref_fill(k, P, Q, xs, ys, xc.size, xc if xc.size else np.zeros(1),
+                  yc if yc.size else np.zeros(1), M, B) < 0:
+        return None
+    return M.reshape(nt, nt).T.copy(), B[:nt * xc.size].reshape(xc.size, nt).T.copy()
+
+
+def system(s, x, y, idx, P, Q=None, ops=OP_LAPLACE | OP_DX | OP_DY, xc=None, yc=None,
+           scale=True, period=None):
+    """The oracle's augmented system of stencil s as its elimination receives
+    it: (xs, ys, a, e) with the local coordinates, a = row-major n x (n+nrhs)
+    (polynomial block first, right-hand sides last) and the scale exponent."""
+    x, y, idx = _f64(x), _f64(y), _i32(idx)
+    k = idx.size
+    Q = 2 * P - 1 if Q is None else Q
+    nc = 0 if xc is None else len(xc)
+    nrhs = num_rhs(ops, nc)
+    n = k + npoly(P)
+    xs, ys = np.empty(k), np.empty(k)
+    a = np.empty(n * (n + nrhs))
+    xcp = None if xc is None else _f64(xc)
+    ycp = None if yc is None else _f64(yc)
+    Lx, Ly = (0.0, 0.0) if period is None else (float(period[0]), float(period[1]))
+    e = lib().orc_system(s, x, y, k, idx, P, Q, ops, nc,
+                         None if xcp is None else xcp.ctypes.data,
+                         None if ycp is None else ycp.ctypes.data, int(bool(scale)), Lx, Ly,
+                         xs, ys, a)
+    if e == -1000:
+        raise ValueError("oracle rejected the arguments")
+    return xs, ys, a.reshape(n, n + nrhs), e
 
 
 def set_threads(n: int) -> None:

@@ -210,42 +210,21 @@ struct Desc {
     double Lx, Ly;     // periods, <= 0 for an open axis
 };
 
-// Assemble one stencil. idx[0..k) are the node indices (idx[0] the
-// centre by convention, but the centre is node s whatever idx holds).
-// Writes w[col][j] = weight of node idx[j] for right-hand side col into
-// out[col] + j. Returns info: 0, or c + 1 for the first zero pivot.
-int assemble_one(const Desc& D, int P, int Q, int s, int k, const int* idx, const double* x,
-                 const double* y, double* const* out, long long out_off,
-                 double* sol_out /* optional n*nrhs, row-major, solution incl. polynomial part */) {
+// The augmented system of one stencil, row-major a[r][c], r < n, c < W =
+// n + nrhs, from the shifted (and scaled) coordinates xs, ys and the scale
+// exponent e. The reference's saddle-point matrix [A P; P^T 0] (fill_matrix,
+// src/rbf_operators.h:123-154) is formed with its polynomial block first:
+// equations [P^T rows (np); node rows (k)], unknowns [lambda (np); w (k)].
+// This relabelling of equations and unknowns fixes the elimination order the
+// CUDA kernel uses; the solution is the reference system's. Right-hand-side
+// column q is column n + q: fill_rhs (src/rbf_operators.h:158-185) for
+// interpolation points, the operator at the centre otherwise.
+void fill_system(const Desc& D, int P, int Q, int k, const double* xs, const double* ys, int e,
+                 const int* col_op, int nrhs, double* a) {
     const int np = npoly(P);
     const int n = k + np;
-    int col_op[kMaxRhs + 64];
-    const int nrhs = rhs_columns(D.ops, D.nc, col_op);
     const int W = n + nrhs;
-
-    double xs[kMaxSys], ys[kMaxSys];
-    // gather + FP64 shift to the stencil centre, src/rbf_operators.h:354-358
-    const double x0 = x[s], y0 = y[s];
-    for (int j = 0; j < k; ++j) {
-        xs[j] = minimum_image(x[idx[j]] - x0, D.Lx);
-        ys[j] = minimum_image(y[idx[j]] - y0, D.Ly);
-    }
-    const int e = D.scale ? scale_exponent(xs, ys, k) : 0;
-    if (e != 0)
-        for (int j = 0; j < k; ++j) {
-            xs[j] = std::ldexp(xs[j], -e);
-            ys[j] = std::ldexp(ys[j], -e);
-        }
-
-    // Augmented system, row-major a[r][c], r < n, c < W. The reference's
-    // saddle-point matrix [A P; P^T 0] (fill_matrix, src/rbf_operators.h:
-    // 123-154) is formed with its polynomial block first: equations
-    // [P^T rows (np); node rows (k)], unknowns [lambda (np); w (k)]. This
-    // relabelling of equations and unknowns fixes the elimination order the
-    // CUDA kernel uses; the solution is the reference system's.
-    static thread_local std::vector<double> abuf;
-    abuf.assign(static_cast<size_t>(n) * W, 0.0);
-    double* a = abuf.data();
+    std::fill(a, a + static_cast<size_t>(n) * W, 0.0);
     for (int i = 0; i < k; ++i) {
         double* row = a + static_cast<size_t>(np + i) * W;
         for (int j = 0; j < k; ++j) {
@@ -260,7 +239,6 @@ int assemble_one(const Desc& D, int P, int Q, int s, int k, const int* idx, cons
             a[m * W + np + i] = b[m];      // P^T block (monomial row m, node i)
         }
     }
-    // right-hand sides
     int ic = 0;
     for (int q = 0; q < nrhs; ++q) {
         const int op = col_op[q];
@@ -283,6 +261,47 @@ int assemble_one(const Desc& D, int P, int Q, int s, int k, const int* idx, cons
             for (int m = 0; m < np; ++m) a[m * W + n + q] = poly_op_at_origin(op, m);
         }
     }
+}
+
+// Gather + FP64 shift to the stencil centre (src/rbf_operators.h:354-358),
+// minimum image in a periodic box, and the power-of-two radius scale.
+// Returns the scale exponent e (0 without scaling).
+int stencil_coords(const Desc& D, int s, int k, const int* idx, const double* x, const double* y,
+                   double* xs, double* ys) {
+    const double x0 = x[s], y0 = y[s];
+    for (int j = 0; j < k; ++j) {
+        xs[j] = minimum_image(x[idx[j]] - x0, D.Lx);
+        ys[j] = minimum_image(y[idx[j]] - y0, D.Ly);
+    }
+    const int e = D.scale ? scale_exponent(xs, ys, k) : 0;
+    if (e != 0)
+        for (int j = 0; j < k; ++j) {
+            xs[j] = std::ldexp(xs[j], -e);
+            ys[j] = std::ldexp(ys[j], -e);
+        }
+    return e;
+}
+
+// Assemble one stencil. idx[0..k) are the node indices (idx[0] the
+// centre by convention, but the centre is node s whatever idx holds).
+// Writes w[col][j] = weight of node idx[j] for right-hand side col into
+// out[col] + j. Returns info: 0, or c + 1 for the first zero pivot.
+int assemble_one(const Desc& D, int P, int Q, int s, int k, const int* idx, const double* x,
+                 const double* y, double* const* out, long long out_off,
+                 double* sol_out /* optional n*nrhs, row-major, solution incl. polynomial part */) {
+    const int np = npoly(P);
+    const int n = k + np;
+    int col_op[kMaxRhs + 64];
+    const int nrhs = rhs_columns(D.ops, D.nc, col_op);
+    const int W = n + nrhs;
+
+    double xs[kMaxSys], ys[kMaxSys];
+    const int e = stencil_coords(D, s, k, idx, x, y, xs, ys);
+
+    static thread_local std::vector<double> abuf;
+    abuf.resize(static_cast<size_t>(n) * W);
+    double* a = abuf.data();
+    fill_system(D, P, Q, k, xs, ys, e, col_op, nrhs, a);
 
     // Gaussian elimination with row-implicit partial pivoting
     bool used[kMaxSys];
@@ -446,6 +465,24 @@ long long orc_assemble_csr(int nstencils, const double* x, const double* y, cons
         bad += (st != 0);
     }
     return err ? -1 : bad;
+}
+
+// One stencil's shifted (and scaled) coordinates xs, ys (k each) and its
+// augmented system as the elimination receives it: row-major n x (n + nrhs),
+// polynomial block first, right-hand sides as the last nrhs columns (see
+// fill_system). Returns the scale exponent, or -1000 on bad arguments. For
+// tests: pins the system against the reference's own fill_matrix/fill_rhs.
+int orc_system(int s, const double* x, const double* y, int k, const int* idx, int P, int Q,
+               int ops, int nc, const double* xc, const double* yc, int scale, double Lx,
+               double Ly, double* xs, double* ys, double* a) {
+    Desc D{ops, nc, xc, yc, scale, Lx, Ly};
+    const int nrhs = check_desc(D, P, Q, k);
+    if (nrhs < 0) return -1000;
+    int col_op[kMaxRhs + 64];
+    rhs_columns(D.ops, D.nc, col_op);
+    const int e = stencil_coords(D, s, k, idx, x, y, xs, ys);
+    fill_system(D, P, Q, k, xs, ys, e, col_op, nrhs, a);
+    return e;
 }
 
 // One stencil's full solution, row-major n x nrhs in the scaled frame:

@@ -1,10 +1,10 @@
 """Regenerates the golden fixtures in tests/golden/ from the reference.
 
-Run in a checkout where the reference is available (``--ref``, default
-``/root/reference``) after ``make -C oracle`` has built the reference's own
-stencil searches (oracle/_ref/libref_knn.so):
+Run where a reference checkout is available (``--ref``, or the environment
+variable ``RBFB_REFERENCE``) after ``make -C oracle`` has built the
+reference's own stencil searches (oracle/_ref/libref_knn.so):
 
-    python tests/golden/make_golden.py
+    RBFB_REFERENCE=<reference checkout> python tests/golden/make_golden.py
 
 Fixtures (numpy .npz, compressed):
 
@@ -26,6 +26,7 @@ Fixtures (numpy .npz, compressed):
 from __future__ import annotations
 
 import argparse
+import os
 import sys
 from pathlib import Path
 
@@ -58,8 +59,11 @@ def read_graph(path):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("RBFB_REFERENCE"),
+                    help="reference checkout (default: $RBFB_REFERENCE)")
     a = ap.parse_args()
+    if not a.ref:
+        ap.error("give --ref or set RBFB_REFERENCE to the reference checkout")
     data = Path(a.ref) / "data"
     for case in ("poisson_32_21", "poisson_32_64", "cartesian_32_21"):
         x, y = read_points(data / f"{case}.points")
