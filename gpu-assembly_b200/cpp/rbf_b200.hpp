@@ -12,8 +12,9 @@
 //                                              187-290): N, NRHS, P, Q as there; ARCH is accepted
 //                                              and ignored (one target, sm_100a)
 //   rbf_b200::assemble_interp_weights<Config>  the kernel of src/rbf_operators.h:320-376, as a host
-//                                              call with the same arguments (device pointers; A is
-//                                              a host array of NRHS device pointers)
+//                                              call with the same arguments, all device pointers:
+//                                              A is the device-resident table of NRHS device
+//                                              pointers the reference kernel dereferences
 //   rbf_b200::laplace_config / assemble_laplace_weights
 //                                              the Laplacian assembly src/main.cpp:15-16,44-45
 //                                              sketches (never implemented there)
@@ -159,8 +160,9 @@ struct interp_config {
 // The reference's kernel assemble_interp_weights<Config> as a host call:
 // nstencils stencils of N neighbours (ja: device, row s at ja[s*N]), weights
 // of interpolation point j (xc[j], yc[j], stencil-local frame, device arrays)
-// into A[j][s*N + k] (A: host array of NRHS device pointers), per-stencil
-// status into info (device, 0 = ok). Asynchronous on `stream`.
+// into A[j][s*N + k], per-stencil status into info (device, 0 = ok). A is,
+// as in the reference (src/rbf_operators.h:324,370-375), a DEVICE array of
+// NRHS device pointers, read by the kernel. Asynchronous on `stream`.
 template <class Config>
 void assemble_interp_weights(int nstencils, const typename Config::value_type* x,
                              const typename Config::value_type* y, const int* ja,
@@ -177,13 +179,16 @@ void assemble_interp_weights(int nstencils, const typename Config::value_type* x
     d.nc = Config::NRHS;
     d.xc = xc;
     d.yc = yc;
-    check(rbfb_assemble(context(), &d, nstencils, x, y, Config::N, ja, A, info, nullptr, stream),
+    check(rbfb_assemble_dtab(context(), &d, nstencils, x, y, Config::N, ja, A, info, nullptr,
+                             stream),
           "assemble_interp_weights");
 }
 
 // The Laplacian assembly src/main.cpp:15-16 names: laplace_config<N, P, Q,
 // ARCH, T> and assemble_laplace_weights<Config>(npoints, x, y, ja, A_tab,
-// info), one right-hand side (the Laplacian at the stencil centre).
+// info), one right-hand side (the Laplacian at the stencil centre); A_tab is
+// a device table of one device pointer, passed as ptr(A_tab) there
+// (src/main.cpp:44-45).
 template <int N_, int P_, int Q_ = 3, unsigned ARCH_ = 1000, typename T_ = double,
           Precision PREC_ = Precision::fp64>
 struct laplace_config : interp_config<N_, 1, P_, Q_, ARCH_, T_, PREC_> {};
@@ -199,7 +204,8 @@ void assemble_laplace_weights(int npoints, const typename Config::value_type* x,
     d.ops = RBFB_OP_LAPLACE;
     d.precision = static_cast<int>(Config::precision);
     d.scale = 1;
-    check(rbfb_assemble(context(), &d, npoints, x, y, Config::N, ja, A_tab, info, nullptr, stream),
+    check(rbfb_assemble_dtab(context(), &d, npoints, x, y, Config::N, ja, A_tab, info, nullptr,
+                             stream),
           "assemble_laplace_weights");
 }
 

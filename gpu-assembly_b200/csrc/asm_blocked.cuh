@@ -476,7 +476,7 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
     // ---- scatter, src/rbf_operators.h:368-375
     const bool bad = info != 0;
     for (int q = 0; q < p.nrhs; ++q) {
-        double* dst = p.values[q] + off;
+        double* dst = out_column(p, q) + off;
         const int sh = -op_order(p.col_op[q]) * e;
         for (int j = lane; j < ks; j += G) {
             const double v = static_cast<double>(X[(NP + j) * NRHS + q]);

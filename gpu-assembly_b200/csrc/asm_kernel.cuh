@@ -81,6 +81,7 @@ struct AsmParams {
     const double* xc;
     const double* yc;
     double* values[kMaxRhs];
+    double* const* values_dev;  // the same table in device memory (read when set)
     int* info;
     // refinement (MIXED)
     int max_sweeps;
@@ -91,6 +92,12 @@ struct AsmParams {
     int* sweeps_max;
     int* work;  // dynamic work counter, or nullptr for a static stride
 };
+
+// Output array of right-hand side q: from the device-resident table when the
+// caller passed one (the reference's T* const* A), else from the parameters.
+__device__ __forceinline__ double* out_column(const AsmParams& p, int q) {
+    return p.values_dev ? p.values_dev[q] : p.values[q];
+}
 
 // Asynchronous global -> shared copies (cp.async, no register staging):
 // the next stencil's data is fetched while the current one is solved.
@@ -878,7 +885,7 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, int sn, 
         // ---- scatter, src/rbf_operators.h:368-375
         const bool bad = info != 0;
         for (int q = 0; q < nrhs; ++q) {
-            double* dst = p.values[q] + off;
+            double* dst = out_column(p, q) + off;
             const int sh = -op_order(p.col_op[q]) * e;
             for (int j = lg; j < ks; j += G) {
                 const double v = static_cast<double>(X[(NP + j) * NRHS + q]);
@@ -1018,7 +1025,7 @@ __device__ __forceinline__ void assemble_one(const AsmParams& p, int s, int sn, 
             }
         } else {
             for (int q = 0; q < nrhs; ++q) {
-                double* dst = p.values[q] + off;
+                double* dst = out_column(p, q) + off;
                 const int sh = -op_order(p.col_op[q]) * e;
                 for (int j = lg; j < ks; j += G) dst[j] = scalbn(x64[(NP + j) * NRHS + q], sh);
             }

@@ -3,9 +3,14 @@
 //   solve_dp              extern "C" __global__ kernel with the reference's
 //                         signature (src/rbf_operators.cpp:7-11): one 15x15
 //                         system, 9 right-hand sides, FP64, <<<1, 32>>>;
-//   rbfb_fill_matrices    fill_matrix / the Fortran fill_kernel
-//                         (src/rbf_operators.h:116-154, src/rbf_cuda.f90:36-99);
-//   rbfb_store_to_csr     the Fortran store_to_csr (src/rbf_cuda.f90:139-157).
+//   rbfb_fill_matrices    fill_matrix (src/rbf_operators.h:116-154) in the
+//                         shifted (and scaled) frame of the assembly;
+//   rbfb_fill_kernel      the Fortran fill_kernel (src/rbf_cuda.f90:36-99):
+//                         degree 2, r^3, absolute coordinates;
+//   rbfb_fill_rhs         the Fortran fill_rhs (src/rbf_cuda.f90:101-136);
+//   rbfb_store_to_csr     the Fortran store_to_csr (src/rbf_cuda.f90:139-157)
+//                         over every stencil, rbfb_store_to_csr_stencil for
+//                         one stencil with its arguments.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -98,10 +103,12 @@ namespace rbfb {
 // ---- fill_matrix ------------------------------------------------------------------
 // One warp per stencil; M + s*ldm*ldm is the column-major saddle-point matrix
 // [A P; P^T 0] of stencil s in the reference's layout and arithmetic order.
+// shift = 0 fills from the absolute coordinates, as the Fortran fill_kernel
+// does (subtracting a zero centre is exact).
 template <int P>
 __global__ void fill_kernel(int nstencils, const double* x, const double* y, const int* ia,
                             const int* ja, int Q, int scale, double Lx, double Ly, double* M,
-                            int ldm) {
+                            int ldm, int shift) {
     const int lane = threadIdx.x & 31;
     const int wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nw = (gridDim.x * blockDim.x) >> 5;
@@ -110,7 +117,7 @@ __global__ void fill_kernel(int nstencils, const double* x, const double* y, con
         const int off = ia[s], k = ia[s + 1] - ia[s];
         if (k < 1 || k + NP > ldm) continue;  // does not fit its slab: left untouched
         double* Ms = M + static_cast<size_t>(s) * ldm * ldm;
-        const double x0 = x[s], y0 = y[s];
+        const double x0 = shift ? x[s] : 0.0, y0 = shift ? y[s] : 0.0;
         int emax = -100000;
         for (int j = lane; j < k; j += 32) {
             const int nb = ja[off + j];
@@ -161,6 +168,34 @@ __global__ void fill_kernel(int nstencils, const double* x, const double* y, con
     }
 }
 
+// The Fortran fill_rhs: B(k, j) = |(xc_j, yc_j) - (x_k, y_k)|^3 for the n
+// stencil nodes, B(n + i, j) = monomial i (degree 2) at (xc_j, yc_j);
+// column-major with leading dimension ldb. One warp per column.
+__global__ void fill_rhs_kernel(int n, const double* x, const double* y, int nc, const double* xc,
+                                const double* yc, double* B, int ldb) {
+    const int lane = threadIdx.x & 31;
+    const int wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int j = wg; j < nc; j += nw) {
+        double* Bj = B + static_cast<size_t>(j) * ldb;
+        const double xe = xc[j], ye = yc[j];
+        for (int k = lane; k < n; k += 32) Bj[k] = phs64<3>(dist2(dsub(xe, x[k]), dsub(ye, y[k])));
+        if (lane == 0) {
+            double mon[6];
+            monomials<2>(xe, ye, mon);
+            for (int m = 0; m < 6; ++m) Bj[n + m] = mon[m];
+        }
+    }
+}
+
+// The Fortran store_to_csr for stencil idx: va[ia[idx] + k] = W(k,1) + W(k,2)
+// for the stencil's nodes, W column-major with leading dimension ldw.
+__global__ void store_to_csr_one_kernel(const int* ia, double* va, const double* W, int ldw,
+                                        int idx) {
+    const int a = ia[idx], n = ia[idx + 1] - a;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) va[a + k] = W[k] + W[k + ldw];
+}
+
 __global__ void store_to_csr_kernel(int nstencils, const int* ia, const double* wxx,
                                      const double* wyy, double* va) {
     const int nnz = ia[nstencils] - ia[0];
@@ -196,15 +231,47 @@ int rbfb_fill_matrices(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, cons
     const int blocks = std::max(1, std::min((nstencils + 3) / 4, ctx->sms * 8));
     const double Lx = desc->period[0], Ly = desc->period[1];
     switch (P) {
-        case 0: fill_kernel<0><<<blocks, 128, 0, st>>>(nstencils, x, y, ia, ja, Q, desc->scale, Lx, Ly, M, ldm); break;
-        case 1: fill_kernel<1><<<blocks, 128, 0, st>>>(nstencils, x, y, ia, ja, Q, desc->scale, Lx, Ly, M, ldm); break;
-        case 2: fill_kernel<2><<<blocks, 128, 0, st>>>(nstencils, x, y, ia, ja, Q, desc->scale, Lx, Ly, M, ldm); break;
-        case 3: fill_kernel<3><<<blocks, 128, 0, st>>>(nstencils, x, y, ia, ja, Q, desc->scale, Lx, Ly, M, ldm); break;
-        default: fill_kernel<4><<<blocks, 128, 0, st>>>(nstencils, x, y, ia, ja, Q, desc->scale, Lx, Ly, M, ldm); break;
+        case 0: fill_kernel<0><<<blocks, 128, 0, st>>>(nstencils, x, y, ia, ja, Q, desc->scale, Lx, Ly, M, ldm, 1); break;
+        case 1: fill_kernel<1><<<blocks, 128, 0, st>>>(nstencils, x, y, ia, ja, Q, desc->scale, Lx, Ly, M, ldm, 1); break;
+        case 2: fill_kernel<2><<<blocks, 128, 0, st>>>(nstencils, x, y, ia, ja, Q, desc->scale, Lx, Ly, M, ldm, 1); break;
+        case 3: fill_kernel<3><<<blocks, 128, 0, st>>>(nstencils, x, y, ia, ja, Q, desc->scale, Lx, Ly, M, ldm, 1); break;
+        default: fill_kernel<4><<<blocks, 128, 0, st>>>(nstencils, x, y, ia, ja, Q, desc->scale, Lx, Ly, M, ldm, 1); break;
     }
     ctx->launches += 1;
     RBFB_CUDA(ctx, cudaGetLastError());
     return RBFB_OK;
+}
+
+int rbfb_fill_kernel(int nstencils, const double* x, const double* y, const int* ia,
+                     const int* ja, double* M, int ldm, void* stream) {
+    if (!x || !y || !ia || !ja || !M) return RBFB_EINVAL;
+    if (nstencils < 0 || ldm < 1) return RBFB_EINVAL;
+    if (nstencils == 0) return RBFB_OK;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return RBFB_ECUDA;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int blocks = std::max(1, std::min((nstencils + 3) / 4, std::max(sms, 1) * 8));
+    fill_kernel<2><<<blocks, 128, 0, static_cast<cudaStream_t>(stream)>>>(
+        nstencils, x, y, ia, ja, 3, 0, 0.0, 0.0, M, ldm, 0);
+    return cudaGetLastError() == cudaSuccess ? RBFB_OK : RBFB_ECUDA;
+}
+
+int rbfb_fill_rhs(int n, const double* x, const double* y, int nc, const double* xc,
+                  const double* yc, double* B, int ldb, void* stream) {
+    if (n < 0 || nc < 0 || ldb < n + 6) return RBFB_EINVAL;
+    if (nc == 0) return RBFB_OK;
+    if (!x || !y || !xc || !yc || !B) return RBFB_EINVAL;
+    const int blocks = std::max(1, std::min((nc + 3) / 4, 1024));
+    fill_rhs_kernel<<<blocks, 128, 0, static_cast<cudaStream_t>(stream)>>>(n, x, y, nc, xc, yc, B,
+                                                                           ldb);
+    return cudaGetLastError() == cudaSuccess ? RBFB_OK : RBFB_ECUDA;
+}
+
+int rbfb_store_to_csr_stencil(int nstencils, const int* ia, double* va, const double* W, int ldw,
+                              int idx, void* stream) {
+    if (!ia || !va || !W || idx < 0 || idx >= nstencils || ldw < 1) return RBFB_EINVAL;
+    store_to_csr_one_kernel<<<1, 128, 0, static_cast<cudaStream_t>(stream)>>>(ia, va, W, ldw, idx);
+    return cudaGetLastError() == cudaSuccess ? RBFB_OK : RBFB_ECUDA;
 }
 
 int rbfb_store_to_csr(int nstencils, const int* ia, const double* wxx, const double* wyy,

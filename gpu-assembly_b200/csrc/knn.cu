@@ -727,6 +727,23 @@ static __device__ __align__(256) unsigned char g_knn_static[kS_total];
 namespace {
 std::mutex g_static_mu;
 void* g_static_addr[64] = {};  // device address of the array, per device ordinal
+
+// The array's device address on the current device: looked up once per
+// device (cudaGetSymbolAddress, with that device current) and cached for the
+// process. A cudaDeviceReset ends the context the address belongs to, so
+// these entry points must not be used across one. nullptr on failure.
+unsigned char* static_scratch(int* dev_out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+    *dev_out = dev;
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_addr[dev]) {
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_knn_static) != cudaSuccess || !p) return nullptr;
+        g_static_addr[dev] = p;
+    }
+    return static_cast<unsigned char*>(g_static_addr[dev]);
+}
 }  // namespace
 
 }  // namespace knn
@@ -735,8 +752,10 @@ void* g_static_addr[64] = {};  // device address of the array, per device ordina
 extern "C" int rbfb_knn_stencils_static(int n, const double* x, const double* y, int k,
                                         const double* period_h, int* ja, void* stream) {
     using namespace rbfb::knn;
+    // the argument checks (and codes) of rbfb_knn_stencils
     if (!x || !y || !ja) return RBFB_EINVAL;
-    if (n < 1 || k < 1 || k > n || k > kMaxK) return RBFB_EINVAL;
+    if (n < 1 || k < 1 || k > n) return RBFB_EINVAL;
+    if (k > kMaxK) return RBFB_EUNSUPPORTED;
     const bool periodic = period_h && period_h[0] > 0 && period_h[1] > 0;
     if (period_h && ((period_h[0] > 0) != (period_h[1] > 0))) return RBFB_EINVAL;
     if (n > kStaticMaxNodes) return RBFB_ETOOBIG;
@@ -752,19 +771,9 @@ extern "C" int rbfb_knn_stencils_static(int n, const double* x, const double* y,
     }
     const long long cells = static_cast<long long>(cx) * cy;
     if (cells > kStaticMaxCells) return RBFB_ETOOBIG;
-    // set-up, once per device, with that device current
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return RBFB_ECUDA;
-    unsigned char* base = nullptr;
-    {
-        std::lock_guard<std::mutex> lock(g_static_mu);
-        if (!g_static_addr[dev]) {
-            void* p = nullptr;
-            if (cudaGetSymbolAddress(&p, g_knn_static) != cudaSuccess || !p) return RBFB_ECUDA;
-            g_static_addr[dev] = p;
-        }
-        base = static_cast<unsigned char*>(g_static_addr[dev]);
-    }
+    unsigned char* base = static_scratch(&dev);
+    if (!base) return RBFB_ECUDA;
     int* cell_of = reinterpret_cast<int*>(base + kS_cell_of);
     int* count = reinterpret_cast<int*>(base + kS_count);
     int* start = reinterpret_cast<int*>(base + kS_start);
@@ -819,4 +828,20 @@ extern "C" int rbfb_knn_stencils_static(int n, const double* x, const double* y,
     const int qblocks = std::max(1, std::min((n + kWarps - 1) / kWarps, std::max(sms, 1) * 16));
     query_kernel<<<qblocks, kWarps * 32, 0, st>>>(a);
     return cudaGetLastError() == cudaSuccess ? RBFB_OK : RBFB_ECUDA;
+}
+
+// Completion status of the last rbfb_knn_stencils_static search on the
+// current device: reads the status word of the fixed array into a host
+// local (no allocation) and synchronises `stream`.
+extern "C" int rbfb_knn_static_status(void* stream) {
+    int dev = 0;
+    unsigned char* base = rbfb::knn::static_scratch(&dev);
+    if (!base) return RBFB_ECUDA;
+    int h = 0;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (cudaMemcpyAsync(&h, base + rbfb::knn::kS_status, sizeof(int), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return RBFB_ECUDA;
+    return h;
 }

@@ -158,14 +158,20 @@ namespace {
 
 // Common set-up of the parameters of one call.
 int base_params(rbfb_ctx* ctx, const rbfb_desc* d, int nstencils, const double* x, const double* y,
-                const int* ja, double* const* values_h, int* info, DevCounters* ctr, AsmParams& p) {
+                const int* ja, double* const* values_h, double* const* values_d, int* info,
+                DevCounters* ctr, AsmParams& p) {
     std::memset(&p, 0, sizeof(p));
     int rc = rhs_columns(d, p);
     if (rc < 0) return fail(ctx, rc, "bad operator mask / interpolation points");
-    if (!x || !y || !ja || !values_h) return fail(ctx, RBFB_EINVAL, "null pointer argument");
-    for (int q = 0; q < p.nrhs; ++q) {
-        if (!values_h[q]) return fail(ctx, RBFB_EINVAL, "null values pointer");
-        p.values[q] = values_h[q];
+    if (!x || !y || !ja || (!values_h && !values_d))
+        return fail(ctx, RBFB_EINVAL, "null pointer argument");
+    if (values_d) {
+        p.values_dev = values_d;  // read by the kernels
+    } else {
+        for (int q = 0; q < p.nrhs; ++q) {
+            if (!values_h[q]) return fail(ctx, RBFB_EINVAL, "null values pointer");
+            p.values[q] = values_h[q];
+        }
     }
     p.nitems = nstencils;
     p.x = x;
@@ -216,7 +222,8 @@ struct EventPair {
 
 int enqueue_fixed(rbfb_ctx* ctx, const rbfb_desc* desc, int first, int count, const double* x,
                   const double* y, int k, const int* ja, double* const* values, int* info,
-                  DevCounters* ctr, int* fb, cudaStream_t st, int row_base) {
+                  DevCounters* ctr, int* fb, cudaStream_t st, int row_base,
+                  double* const* values_d) {
     const int P = desc->degree;
     const int Q = desc->phs ? desc->phs : 2 * P - 1;
     const int n = k + npoly(P);
@@ -227,7 +234,7 @@ int enqueue_fixed(rbfb_ctx* ctx, const rbfb_desc* desc, int first, int count, co
                     "no compiled kernel for P=" + std::to_string(P) + " Q=" + std::to_string(Q) +
                         " n=" + std::to_string(n));
     AsmParams p;
-    int rc = base_params(ctx, desc, count, x, y, ja, values, info, ctr, p);
+    int rc = base_params(ctx, desc, count, x, y, ja, values, values_d, info, ctr, p);
     if (rc) return rc;
     if (p.nrhs > variants()[v].nrhs)
         return fail(ctx, RBFB_EUNSUPPORTED, "more right-hand sides than the compiled kernels hold");
@@ -318,9 +325,11 @@ int rbfb_destroy(rbfb_ctx* ctx) {
     return RBFB_OK;
 }
 
-int rbfb_assemble(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const double* x,
-                  const double* y, int k, const int* ja, double* const* values_h, int* info,
-                  rbfb_stats* stats, void* stream) {
+namespace {
+
+int assemble_fixed_call(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const double* x,
+                        const double* y, int k, const int* ja, double* const* values_h,
+                        double* const* values_d, int* info, rbfb_stats* stats, void* stream) {
     if (!ctx) return RBFB_EINVAL;
     std::lock_guard<std::mutex> lock(ctx->mu);
     int rc = check_desc(ctx, desc);
@@ -340,9 +349,26 @@ int rbfb_assemble(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const dou
         if (rc) return rc;
     }
     rc = enqueue_fixed(ctx, desc, 0, nstencils, x, y, k, ja, values_h, info, ctx->ctr,
-                       ctx->fb_list, st);
+                       ctx->fb_list, st, 0, values_d);
     if (rc) return rc;
     return finish_stats(ctx, info, nstencils, stats, st, ev.a, ev.b, 1);
+}
+
+}  // namespace
+
+int rbfb_assemble(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const double* x,
+                  const double* y, int k, const int* ja, double* const* values_h, int* info,
+                  rbfb_stats* stats, void* stream) {
+    return assemble_fixed_call(ctx, desc, nstencils, x, y, k, ja, values_h, nullptr, info, stats,
+                               stream);
+}
+
+int rbfb_assemble_dtab(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const double* x,
+                       const double* y, int k, const int* ja, double* const* values_d, int* info,
+                       rbfb_stats* stats, void* stream) {
+    if (!values_d) return ctx ? fail(ctx, RBFB_EINVAL, "null values table") : RBFB_EINVAL;
+    return assemble_fixed_call(ctx, desc, nstencils, x, y, k, ja, nullptr, values_d, info, stats,
+                               stream);
 }
 
 int rbfb_assemble_range(rbfb_ctx* ctx, const rbfb_desc* desc, int first, int count, int n,

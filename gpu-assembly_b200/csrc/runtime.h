@@ -90,9 +90,12 @@ int count_singular(rbfb_ctx* ctx, const int* info, int n, unsigned long long* ou
 
 // Fixed-width assembly of stencils [first, first + count) on `st` with the
 // counters `ctr` and the fallback region fb (count entries). No sync.
+// values: host table of device pointers, or nullptr when values_d (a table in
+// device memory) is given.
 int enqueue_fixed(rbfb_ctx* ctx, const rbfb_desc* desc, int first, int count, const double* x,
                   const double* y, int k, const int* ja, double* const* values, int* info,
-                  DevCounters* ctr, int* fb, cudaStream_t st, int row_base = 0);
+                  DevCounters* ctr, int* fb, cudaStream_t st, int row_base = 0,
+                  double* const* values_d = nullptr);
 
 int check_desc(rbfb_ctx* ctx, const rbfb_desc* d);
 

@@ -239,8 +239,9 @@ __global__ void __launch_bounds__(kThreads, kBlocksPerSm) p_kernel(Args a) {
     const State* st = a.st;
     if (st->done) return;
     const double beta = st->beta, omega = st->omega;
-    const int stride = gridDim.x * kThreads;
-    for (int s = blockIdx.x * kThreads + threadIdx.x; s < a.n; s += stride)
+    const long long stride = static_cast<long long>(gridDim.x) * kThreads;
+    for (long long s = static_cast<long long>(blockIdx.x) * kThreads + threadIdx.x; s < a.n;
+         s += stride)
         a.p[s] = fma(beta, fma(-omega, a.v[s], a.p[s]), a.r[s]);
 }
 
@@ -270,8 +271,9 @@ __global__ void __launch_bounds__(kThreads, kBlocksPerSm) s_kernel(Args a) {
     const State* st = a.st;
     if (st->done) return;
     const double alpha = st->alpha;
-    const int stride = gridDim.x * kThreads;
-    for (int i = blockIdx.x * kThreads + threadIdx.x; i < a.n; i += stride)
+    const long long stride = static_cast<long long>(gridDim.x) * kThreads;
+    for (long long i = static_cast<long long>(blockIdx.x) * kThreads + threadIdx.x; i < a.n;
+         i += stride)
         a.s[i] = fma(-alpha, a.v[i], a.r[i]);
 }
 
@@ -308,8 +310,9 @@ __global__ void __launch_bounds__(kThreads, kBlocksPerSm) update_kernel(Args a) 
     if (st->done) return;
     const double alpha = st->alpha, omega = st->omega;
     double acc[2] = {0.0, 0.0};
-    const int stride = gridDim.x * kThreads;
-    for (int i = blockIdx.x * kThreads + threadIdx.x; i < a.n; i += stride) {
+    const long long stride = static_cast<long long>(gridDim.x) * kThreads;
+    for (long long i = static_cast<long long>(blockIdx.x) * kThreads + threadIdx.x; i < a.n;
+         i += stride) {
         const double si = a.s[i];
         a.u[i] = fma(omega, si, fma(alpha, a.p[i], a.u[i]));
         const double ri = fma(-omega, a.t[i], si);

@@ -90,8 +90,11 @@ _PROTOS = {
     "rbfb_knn_query": (_i, [_vp, _i, _vp, _vp, _i, _vp, _vp, _i, _vp, _vp, _vp]),
     "rbfb_knn_status": (_i, [_vp, _vp]),
     "rbfb_knn_stencils_static": (_i, [_i, _vp, _vp, _i, _vp, _vp, _vp]),
+    "rbfb_knn_static_status": (_i, [_vp]),
     "rbfb_assemble": (_i, [_vp, C.POINTER(Desc), _i, _vp, _vp, _i, _vp, _vp, _vp,
                            C.POINTER(Stats), _vp]),
+    "rbfb_assemble_dtab": (_i, [_vp, C.POINTER(Desc), _i, _vp, _vp, _i, _vp, _vp, _vp,
+                                C.POINTER(Stats), _vp]),
     "rbfb_assemble_range": (_i, [_vp, C.POINTER(Desc), _i, _i, _i, _vp, _vp, _i, _vp, _vp, _vp,
                                  C.POINTER(Stats), _vp]),
     "rbfb_assemble_csr": (_i, [_vp, C.POINTER(Desc), _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
@@ -100,6 +103,9 @@ _PROTOS = {
                                 C.POINTER(Stats)]),
     "rbfb_fill_matrices": (_i, [_vp, C.POINTER(Desc), _i, _vp, _vp, _vp, _vp, _vp, _i, _vp]),
     "rbfb_store_to_csr": (_i, [_i, _vp, _vp, _vp, _vp, _vp]),
+    "rbfb_fill_kernel": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _i, _vp]),
+    "rbfb_fill_rhs": (_i, [_i, _vp, _vp, _i, _vp, _vp, _vp, _i, _vp]),
+    "rbfb_store_to_csr_stencil": (_i, [_i, _vp, _vp, _vp, _i, _i, _vp]),
     "rbfb_spmv": (_i, [_i, _i, _vp, _vp, _vp, _vp, _vp, _i, _vp]),
     "rbfb_solve_bicgstab": (_i, [_vp, _i, _i, _vp, _vp, _vp, _vp, _i, _vp, _vp, _d, _i,
                                  C.POINTER(_i), C.POINTER(_d), _vp]),
@@ -279,6 +285,18 @@ class Context:
         self._check(st, "assemble")
         return s.as_dict() if s is not None else None
 
+    def assemble_dtab(self, desc: Desc, x, y, k, ja, values_tab, info=None, stats=False,
+                      stream=None):
+        """rbfb_assemble with the output pointer table in device memory
+        (values_tab: an int64 device tensor of nrhs device pointers)."""
+        n = x.numel()
+        s = Stats() if stats else None
+        st = lib().rbfb_assemble_dtab(self.h, C.byref(desc), n, _ptr(x), _ptr(y), k, _ptr(ja),
+                                      _ptr(values_tab), _ptr(info),
+                                      C.byref(s) if s is not None else None, _stream(stream))
+        self._check(st, "assemble_dtab")
+        return s.as_dict() if s is not None else None
+
     def assemble_range(self, desc: Desc, first, count, x, y, k, ja_rows, values_rows,
                        info_rows=None, stats=False, stream=None):
         """Stencils first..first+count-1 of the node set (x, y): ja_rows and
@@ -373,6 +391,15 @@ def knn_stencils_static(x, y, k, ja, period=None, stream=None):
         raise RbfError(st, status_string(st))
 
 
+def knn_static_status(stream=None) -> int:
+    """rbfb_knn_static_status: 0 when the last no-allocation search on the
+    current device finished every query, 1 when one gave up. Synchronises."""
+    st = lib().rbfb_knn_static_status(_stream(stream))
+    if st < 0:
+        raise RbfError(st, status_string(st))
+    return st
+
+
 def variant_name(index: int):
     v = lib().rbfb_variant_name(index)
     return None if v is None else v.decode()
@@ -416,6 +443,31 @@ def store_to_csr(nstencils, ia, wxx, wyy, va, stream=None):
                                  _stream(stream))
     if st != OK:
         raise RbfError(st, "store_to_csr")
+
+
+def fill_kernel(nstencils, x, y, ia, ja, M, ldm, stream=None):
+    """rbfb_fill_kernel: the Fortran fill_kernel (degree 2, r^3, absolute
+    coordinates), stencil s's matrix at M[s*ldm*ldm:]."""
+    st = lib().rbfb_fill_kernel(nstencils, _ptr(x), _ptr(y), _ptr(ia), _ptr(ja), _ptr(M), ldm,
+                                _stream(stream))
+    if st != OK:
+        raise RbfError(st, "fill_kernel")
+
+
+def fill_rhs(n, x, y, xc, yc, B, ldb, stream=None):
+    """rbfb_fill_rhs: the Fortran fill_rhs (interpolation right-hand sides)."""
+    st = lib().rbfb_fill_rhs(n, _ptr(x), _ptr(y), xc.numel(), _ptr(xc), _ptr(yc), _ptr(B), ldb,
+                             _stream(stream))
+    if st != OK:
+        raise RbfError(st, "fill_rhs")
+
+
+def store_to_csr_stencil(nstencils, ia, va, W, ldw, idx, stream=None):
+    """rbfb_store_to_csr_stencil: the Fortran store_to_csr for stencil idx."""
+    st = lib().rbfb_store_to_csr_stencil(nstencils, _ptr(ia), _ptr(va), _ptr(W), ldw, idx,
+                                         _stream(stream))
+    if st != OK:
+        raise RbfError(st, "store_to_csr_stencil")
 
 
 def solve_dp(A, ipiv, B, info, stream=None):

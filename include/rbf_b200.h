@@ -138,12 +138,23 @@ int rbfb_knn_query(rbfb_ctx* ctx, int n, const double* x, const double* y, int n
  * Limit: n <= 65,536 nodes (and a cell grid of at most n/2 cells); larger
  * problems are rejected with RBFB_ETOOBIG. The first call on a device looks
  * up the array's device address (cudaGetSymbolAddress) with that device
- * current; make that first call before any stream capture. All calls share
- * the one array: calls whose work overlaps on the GPU (other streams, other
- * host threads) race and must be serialised by the caller. Same arguments,
- * result and ordering as rbfb_knn_stencils. */
+ * current; make that first call before any stream capture. The address is
+ * kept for the life of the process, so do not use these entry points across
+ * a cudaDeviceReset. All calls share the one array: calls whose work
+ * overlaps on the GPU (other streams, other host threads) race and must be
+ * serialised by the caller. Same arguments, argument checks (and status
+ * codes), result and ordering as rbfb_knn_stencils; like it, a query that
+ * gives up widening its search leaves its row of ja unwritten, which
+ * rbfb_knn_static_status reports. */
 int rbfb_knn_stencils_static(int n, const double* x, const double* y, int k,
                              const double* period_h, int* ja, void* stream);
+
+/* Completion status of the last rbfb_knn_stencils_static search on the
+ * current device: 0 when every query finished, 1 when a query gave up (its
+ * row of ja is then unwritten), negative on a CUDA error. Reads the status
+ * word of the fixed array into host memory, allocating nothing, and
+ * synchronises `stream`. No reference counterpart. */
+int rbfb_knn_static_status(void* stream);
 
 /* Completion status of the last search on this context: 0 when every query
  * finished, 1 when a query gave up widening its search (its row of ja is
@@ -161,6 +172,15 @@ int rbfb_knn_status(rbfb_ctx* ctx, void* stream);
 int rbfb_assemble(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const double* x,
                   const double* y, int k, const int* ja, double* const* values_h, int* info,
                   rbfb_stats* stats, void* stream);
+
+/* rbfb_assemble with the pointer table in DEVICE memory, as the reference's
+ * kernel takes it: `T* const* A`, dereferenced on the device
+ * (src/rbf_operators.h:324,370-375), filled by the caller and passed as
+ * ptr(A_tab) (src/main.cpp:44-45). values_d holds nrhs device pointers; the
+ * kernels read it, so the call stays asynchronous. */
+int rbfb_assemble_dtab(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const double* x,
+                       const double* y, int k, const int* ja, double* const* values_d, int* info,
+                       rbfb_stats* stats, void* stream);
 
 /* Stencils first .. first+count-1 of an n-node set (all n coordinates given):
  * ja_rows, values_rows[q] and info_rows hold only those rows (row first at
@@ -204,6 +224,31 @@ int rbfb_assemble_host(rbfb_ctx* ctx, const rbfb_desc* desc, int n, const double
 int rbfb_fill_matrices(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const double* x,
                        const double* y, const int* ia, const int* ja, double* M, int ldm,
                        void* stream);
+
+/* The Fortran fill_kernel (src/rbf_cuda.f90:36-99) with its arguments: the
+ * degree-2, r^3 saddle-point matrix of each CSR stencil (0-based ia, ja), from
+ * the ABSOLUTE node coordinates (no shift, no scaling), column-major with
+ * leading dimension ldm, stencil s in the ldm x ldm slab at M + s*ldm*ldm
+ * (a stencil with k_s + 6 > ldm is skipped). For nstencils = 1 this is the
+ * reference's single output matrix (its kernel writes every stencil into the
+ * same M). Arithmetic as there: (x_col - x_k)^2 + (y_col - y_k)^2, then
+ * r2 * sqrt(r2). No context. */
+int rbfb_fill_kernel(int nstencils, const double* x, const double* y, const int* ia,
+                     const int* ja, double* M, int ldm, void* stream);
+
+/* The Fortran fill_rhs (src/rbf_cuda.f90:101-136) with its arguments:
+ * B(k, j) = |(xc_j, yc_j) - (x_k, y_k)|^3 for the n stencil nodes (x, y hold
+ * the stencil's own coordinates) and B(n + i, j) = the i-th degree-2 monomial
+ * at (xc_j, yc_j), for j < nc; column-major, ldb >= n + 6. No context. */
+int rbfb_fill_rhs(int n, const double* x, const double* y, int nc, const double* xc,
+                  const double* yc, double* B, int ldb, void* stream);
+
+/* The Fortran store_to_csr (src/rbf_cuda.f90:139-157) with its arguments, for
+ * one stencil idx: va[ia[idx] + k] = W(k,1) + W(k,2), k < ia[idx+1] - ia[idx],
+ * W column-major with leading dimension ldw (p_xx + p_yy). The reference's is
+ * a device subroutine; this is a host call launching one small kernel. */
+int rbfb_store_to_csr_stencil(int nstencils, const int* ia, double* va, const double* W, int ldw,
+                              int idx, void* stream);
 
 /* va[ia[s] + j] = W[s][j][0] + W[s][j][1]: the Fortran store_to_csr, which
  * forms a Laplacian from the d2/dx2 and d2/dy2 weight columns (src/rbf_cuda.f90:

@@ -56,7 +56,7 @@ def lib():
                                         C.c_double, _dp, C.c_void_p]
         L.orc_fill_matrix.restype = C.c_int
         L.orc_fill_matrix.argtypes = [C.c_int, _dp, _dp, C.c_int, _ip, C.c_int, C.c_int, C.c_int,
-                                      C.c_double, C.c_double, _dp, C.c_int]
+                                      C.c_double, C.c_double, _dp, C.c_int, C.c_int]
         L.orc_knn_brute.restype = C.c_int
         L.orc_knn_brute.argtypes = [C.c_int, _dp, _dp, C.c_int, _dp, _dp, C.c_int, C.c_double,
                                     C.c_double, _ip, C.c_void_p]
@@ -287,16 +287,19 @@ def solve_stencil(s, x, y, idx, P, Q=None, ops=OP_LAPLACE | OP_DX | OP_DY, scale
     return sol.reshape(n, nrhs), info
 
 
-def fill_matrix(s, x, y, idx, P, Q=None, scale=True, period=None):
+def fill_matrix(s, x, y, idx, P, Q=None, scale=True, period=None, shift=True):
     """The reference-layout saddle-point matrix [A P; P^T 0] of one stencil
-    (column-major in the reference; returned as a numpy (n, n) array)."""
+    (column-major in the reference; returned as a numpy (n, n) array);
+    shift=False fills from the absolute coordinates (the Fortran
+    fill_kernel)."""
     x, y, idx = _f64(x), _f64(y), _i32(idx)
     k = idx.size
     Q = 2 * P - 1 if Q is None else Q
     n = k + npoly(P)
     M = np.empty(n * n, np.float64)
     Lx, Ly = (0.0, 0.0) if period is None else (float(period[0]), float(period[1]))
-    e = lib().orc_fill_matrix(s, x, y, k, idx, P, Q, int(bool(scale)), Lx, Ly, M, n)
+    e = lib().orc_fill_matrix(s, x, y, k, idx, P, Q, int(bool(scale)), Lx, Ly, M, n,
+                              int(bool(shift)))
     return M.reshape(n, n).T.copy(), e
 
 

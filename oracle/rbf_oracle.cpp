@@ -497,15 +497,17 @@ int orc_solve_stencil(int s, const double* x, const double* y, int k, const int*
 
 // The saddle-point matrix of one stencil, column-major n x n with leading
 // dimension ldm (fill_matrix's layout, src/rbf_operators.h:116-122), in the
-// shifted frame and, with scale = 1, the scaled one. Returns the scale
-// exponent e.
+// shifted frame and, with scale = 1, the scaled one; with shift = 0 from the
+// absolute coordinates, as the Fortran fill_kernel (src/rbf_cuda.f90:56-70).
+// Returns the scale exponent e.
 int orc_fill_matrix(int s, const double* x, const double* y, int k, const int* idx, int P,
-                    int Q, int scale, double Lx, double Ly, double* M, int ldm) {
+                    int Q, int scale, double Lx, double Ly, double* M, int ldm, int shift) {
     const int np = npoly(P);
     double xs[kMaxSys], ys[kMaxSys];
+    const double x0 = shift ? x[s] : 0.0, y0 = shift ? y[s] : 0.0;
     for (int j = 0; j < k; ++j) {
-        xs[j] = minimum_image(x[idx[j]] - x[s], Lx);
-        ys[j] = minimum_image(y[idx[j]] - y[s], Ly);
+        xs[j] = minimum_image(x[idx[j]] - x0, Lx);
+        ys[j] = minimum_image(y[idx[j]] - y0, Ly);
     }
     const int e = scale ? scale_exponent(xs, ys, k) : 0;
     for (int j = 0; j < k; ++j) {

@@ -37,6 +37,7 @@ def test_static_search_matches_the_ordinary_one(torch_cuda):
             for call in range(2):  # two calls in a row on the same scratch
                 ja = T.full((n * k,), -1, dtype=T.int32, device="cuda")
                 R.knn_stencils_static(xd, yd, k, ja, period=period)
+                assert R.knn_static_status() == 0, f"call {call}: a query gave up"
                 T.cuda.synchronize()
                 np.testing.assert_array_equal(ja.cpu().numpy(), ref.cpu().numpy(),
                                               err_msg=f"call {call}, n={n}, k={k}")
@@ -49,4 +50,28 @@ def test_static_search_rejects_oversize(torch_cuda):
     ja = T.empty(n * 4, dtype=T.int32, device="cuda")
     with pytest.raises(R.RbfError) as e:
         R.knn_stencils_static(x, x, 4, ja)
+    assert e.value.status == R.ETOOBIG
+
+
+def test_static_search_argument_codes(torch_cuda):
+    """The same status codes as the ordinary entry point for the same bad
+    arguments; an extreme periodic aspect ratio overflows the fixed cell grid
+    (ETOOBIG). None of these cases launches a kernel."""
+    T = torch_cuda
+    n = 1000
+    x = T.rand(n, dtype=T.float64, device="cuda")
+    ja = T.empty(n * 130, dtype=T.int32, device="cuda")
+    with R.Context(0) as ctx:
+        for k, period in ((n + 1, None), (129, None), (0, None), (8, (1.0, 0.0))):
+            with pytest.raises(R.RbfError) as e_ord:
+                ctx.knn_stencils(x, x, k, ja, period=period)
+            with pytest.raises(R.RbfError) as e_st:
+                R.knn_stencils_static(x, x, k, ja, period=period)
+            assert e_st.value.status == e_ord.value.status, (k, period)
+    assert R.knn_static_status() == 0  # still the last completed search's
+    m = 60000
+    xm = T.rand(m, dtype=T.float64, device="cuda")
+    jm = T.empty(m * 4, dtype=T.int32, device="cuda")
+    with pytest.raises(R.RbfError) as e:
+        R.knn_stencils_static(xm, xm, 4, jm, period=(1.0e6, 1.0e-6))
     assert e.value.status == R.ETOOBIG
