@@ -82,6 +82,29 @@ def solve_bytes(n, nnz):
     return 24 * nnz + n * (2 * (4 + 1 + 8) + 8 + 8 + 8 + 24 + 32 + 56)
 
 
+def disk_csr(ctx, dev, n=None):
+    """The uneven disk workload on the device: node coordinates, per-node k
+    and degree, and the ragged CSR stencils (the k_s nearest of every node,
+    from one k-NN search at the largest k, trimmed per row)."""
+    c = NS.config_disk_uneven(**({"n": n} if n else {}))
+    x, y = c["x"], c["y"]
+    n = x.size
+    xd, yd = torch.as_tensor(x, device=dev), torch.as_tensor(y, device=dev)
+    kvec = torch.as_tensor(c["kvec"], device=dev)
+    deg = torch.as_tensor(c["degree"], device=dev)
+    kmax = int(kvec.max())
+    jaf = torch.empty(n * kmax, dtype=torch.int32, device=dev)
+    ctx.knn_stencils(xd, yd, kmax, jaf)
+    keep = torch.arange(kmax, device=dev)[None, :] < kvec[:, None]
+    ja = jaf.view(n, kmax)[keep].contiguous()
+    ia = torch.zeros(n + 1, dtype=torch.int32, device=dev)
+    ia[1:] = torch.cumsum(kvec, 0).to(torch.int32)
+    del jaf
+    torch.cuda.synchronize()
+    return dict(c=c, xd=xd, yd=yd, kvec=kvec, deg=deg, ia=ia, ja=ja, n=n, nnz=int(ia[-1]),
+                kmax=kmax)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", choices=["periodic", "disk", "bump"], default="periodic")
@@ -92,6 +115,9 @@ def main(argv=None):
     ap.add_argument("--precision", choices=["fp64", "mixed", "both"], default="mixed")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--tune", action="store_true", help="autotune the shape first")
+    ap.add_argument("--shape", default=None,
+                    help="pin this compiled kernel shape (rbf_b200.variant_names()) for the "
+                         "fixed-width workloads")
     ap.add_argument("--solve", type=int, default=0,
                     help="disk: BiCGSTAB iterations on the assembled Laplacian")
     a = ap.parse_args(argv)
@@ -103,22 +129,10 @@ def main(argv=None):
 
     with R.Context(0) as ctx:
         if a.workload == "disk":
-            c = NS.config_disk_uneven(**({"n": a.n} if a.n else {}))
-            x, y = c["x"], c["y"]
-            n = x.size
-            xd, yd = torch.as_tensor(x, device=dev), torch.as_tensor(y, device=dev)
-            kvec = torch.as_tensor(c["kvec"], device=dev)
-            deg = torch.as_tensor(c["degree"], device=dev)
-            kmax = int(kvec.max())
-            jaf = torch.empty(n * kmax, dtype=torch.int32, device=dev)
-            ctx.knn_stencils(xd, yd, kmax, jaf)
-            keep = torch.arange(kmax, device=dev)[None, :] < kvec[:, None]
-            ja = jaf.view(n, kmax)[keep].contiguous()
-            ia = torch.zeros(n + 1, dtype=torch.int32, device=dev)
-            ia[1:] = torch.cumsum(kvec, 0).to(torch.int32)
-            del jaf
-            nnz = int(ia[-1])
-            torch.cuda.synchronize()
+            w = disk_csr(ctx, dev, a.n)
+            c, xd, yd, ia, ja, deg = w["c"], w["xd"], w["yd"], w["ia"], w["ja"], w["deg"]
+            kvec = w["kvec"]
+            n, nnz, kmax = w["n"], w["nnz"], w["kmax"]
             res = {}
             for f in forms:
                 vals = [torch.empty(nnz, dtype=torch.float64, device=dev) for _ in range(3)]
@@ -176,7 +190,10 @@ def main(argv=None):
                 vals = [torch.empty(n * k, dtype=torch.float64, device=dev) for _ in range(3)]
                 info = torch.empty(n, dtype=torch.int32, device=dev)
                 d = R.make_desc(P, 0, R.DEFAULT_OPS, prec[f], True, period=per)
-                if a.tune:
+                if a.shape:
+                    ctx.select_variant(d, k, R.variant_names().index(a.shape))
+                    shape = a.shape
+                elif a.tune:
                     shape = R.variant_name(ctx.autotune(d, xd, yd, k, ja, vals))
                 ms, st = _events_ms(lambda sts: ctx.assemble(d, xd, yd, k, ja, vals, info, stats=sts,
                                                              stream=stream), a.reps, stream)

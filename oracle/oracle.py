@@ -232,12 +232,14 @@ def assemble(x, y, ja, k, P, Q=None, ops=OP_LAPLACE | OP_DX | OP_DY, xc=None, yc
     return np.stack(out), info
 
 
-def assemble_ld(x, y, ja, k, P, Q=None, ops=OP_LAPLACE | OP_DX | OP_DY, scale=True, period=None):
+def assemble_ld(x, y, ja, k, P, Q=None, ops=OP_LAPLACE | OP_DX | OP_DY, scale=True, period=None,
+                nstencils=None):
     """The same assembly in x87 long double (64-bit significand): a more
     accurate solution to measure FP64 and refined-FP32 errors against on
-    ill-conditioned stencils. Derivative operators only."""
+    ill-conditioned stencils. Derivative operators only. nstencils restricts
+    it to the stencils of the first nodes (ja then holds only their rows)."""
     x, y, ja = _f64(x), _f64(y), _i32(ja)
-    n = x.size
+    n = x.size if nstencils is None else int(nstencils)
     Q = 2 * P - 1 if Q is None else Q
     nrhs = num_rhs(ops, 0)
     out = [np.empty(n * k, np.float64) for _ in range(nrhs)]
