@@ -67,6 +67,7 @@ struct BlkCfg {
     static constexpr int LV0 = (WMAX + VE - 1) / VE;
     static constexpr int LDSV = (LV0 % 2) ? LV0 : LV0 + 1;
     static constexpr int LDS = LDSV * VE;
+    static_assert(((NMAX + PB - 1) / PB) * PB <= LDS, "a row holds every panel's columns");
     static constexpr int al16(int b) { return (b + 15) & ~15; }
     static constexpr int off_cx = 0;
     static constexpr int off_cy = off_cx + al16(8 * KMAX);

@@ -29,3 +29,7 @@ RBFB_VARIANT(mix_p4q7_n64_smem, float, 16, 2, 64, 3, 4, 7, true, 32, 1, true, tr
 RBFB_VARIANT(mix_p4q7_n80_smem, float, 16, 2, 80, 3, 4, 7, true, 32, 1, true, true)
 RBFB_BLK_VARIANT(b64_p3q5_n48_pb8, double, 48, 3, 3, 5, false, 96, 1, 8, true)
 RBFB_BLK_VARIANT(b64_p3q5_n48_pb8w1, double, 48, 3, 3, 5, false, 32, 1, 8, true)
+RBFB_BLK_VARIANT(b64_p2q3_n32_pb8, double, 32, 3, 2, 3, false, 128, 1, 8, true)
+RBFB_BLK_VARIANT(b64_p2q3_n32_r8, double, 32, 8, 2, 3, false, 128, 1, 8, true)
+RBFB_BLK_VARIANT(b64_p4q7_n64_pb8, double, 64, 3, 4, 7, false, 32, 1, 8, true)
+RBFB_BLK_VARIANT(b64_p4q7_n80_pb8, double, 80, 3, 4, 7, false, 32, 1, 8, true)

@@ -59,19 +59,22 @@ int rhs_columns(const rbfb_desc* d, AsmParams& p) {
     return m;
 }
 
-int pick_variant(rbfb_ctx* ctx, bool mixed, int P, int Q, int n) {
+int pick_variant(rbfb_ctx* ctx, bool mixed, int P, int Q, int n, int nrhs) {
     const auto& vs = variants();
+    auto serves = [&](const Variant& v) {
+        return v.mixed == mixed && v.P == P && v.Q == Q && v.nrhs >= nrhs;
+    };
     int best_ntp = 1 << 30;
     for (const auto& v : vs)
-        if (v.mixed == mixed && v.P == P && v.Q == Q && v.ntp >= n) best_ntp = std::min(best_ntp, v.ntp);
+        if (serves(v) && v.ntp >= n) best_ntp = std::min(best_ntp, v.ntp);
     if (best_ntp == (1 << 30)) return -1;
     if (ctx) {
         auto it = ctx->tuned.find({mixed ? 1 : 0, P, Q, best_ntp});
-        if (it != ctx->tuned.end() && it->second.variant >= 0) return it->second.variant;
+        if (it != ctx->tuned.end() && it->second.variant >= 0 && serves(vs[it->second.variant]))
+            return it->second.variant;
     }
     for (size_t i = 0; i < vs.size(); ++i)
-        if (vs[i].mixed == mixed && vs[i].P == P && vs[i].Q == Q && vs[i].ntp == best_ntp)
-            return static_cast<int>(i);
+        if (serves(vs[i]) && vs[i].ntp == best_ntp) return static_cast<int>(i);
     return -1;
 }
 
@@ -228,14 +231,15 @@ int enqueue_fixed(rbfb_ctx* ctx, const rbfb_desc* desc, int first, int count, co
     const int Q = desc->phs ? desc->phs : 2 * P - 1;
     const int n = k + npoly(P);
     const bool mixed = desc->precision == RBFB_FP32_IR;
-    const int v = pick_variant(ctx, mixed, P, Q, n);
-    if (v < 0)
-        return fail(ctx, RBFB_EUNSUPPORTED,
-                    "no compiled kernel for P=" + std::to_string(P) + " Q=" + std::to_string(Q) +
-                        " n=" + std::to_string(n));
     AsmParams p;
     int rc = base_params(ctx, desc, count, x, y, ja, values, values_d, info, ctr, p);
     if (rc) return rc;
+    const int v = pick_variant(ctx, mixed, P, Q, n, p.nrhs);
+    if (v < 0)
+        return fail(ctx, RBFB_EUNSUPPORTED,
+                    "no compiled kernel for P=" + std::to_string(P) + " Q=" + std::to_string(Q) +
+                        " n=" + std::to_string(n) + " with " + std::to_string(p.nrhs) +
+                        " right-hand sides");
     if (p.nrhs > variants()[v].nrhs)
         return fail(ctx, RBFB_EUNSUPPORTED, "more right-hand sides than the compiled kernels hold");
     p.k = k;
@@ -247,7 +251,7 @@ int enqueue_fixed(rbfb_ctx* ctx, const rbfb_desc* desc, int first, int count, co
     rc = launch_variant(ctx, v, p, st);
     if (rc) return rc;
     // FP64 kernel over the stencils whose refinement stalled
-    const int v64 = pick_variant(ctx, false, P, Q, n);
+    const int v64 = pick_variant(ctx, false, P, Q, n, p.nrhs);
     if (v64 < 0) return fail(ctx, RBFB_EUNSUPPORTED, "no FP64 fallback kernel for this shape");
     AsmParams f = p;
     f.list = fb;

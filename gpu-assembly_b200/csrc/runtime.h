@@ -72,9 +72,9 @@ int cuda_fail(rbfb_ctx* ctx, cudaError_t e, const char* where);
 // Fills col_op / col_ic of params from the descriptor; returns nrhs or < 0.
 int rhs_columns(const rbfb_desc* d, AsmParams& p);
 
-// Variant for (mixed, P, Q) that fits a system of n unknowns, honouring the
-// tuned table; -1 when none is compiled.
-int pick_variant(rbfb_ctx* ctx, bool mixed, int P, int Q, int n);
+// Variant for (mixed, P, Q) that fits a system of n unknowns with nrhs
+// right-hand sides, honouring the tuned table; -1 when none is compiled.
+int pick_variant(rbfb_ctx* ctx, bool mixed, int P, int Q, int n, int nrhs = 1);
 
 // Persistent grid size of a variant (blocks), after the shared-memory opt-in.
 int grid_for(rbfb_ctx* ctx, int v, int blocks_per_sm_override = 0);

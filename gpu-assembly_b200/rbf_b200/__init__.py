@@ -116,6 +116,10 @@ _PROTOS = {
     "rbfb_renumber_csr": (_i, [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "rbfb_permute": (_i, [_i, _vp, _vp, _vp, _i, _vp]),
     "rbfb_solve_dp": (_i, [_vp, _vp, _vp, _vp, _vp]),
+    "rbfb_lbm_feq": (_i, [_i, _i, _vp, _vp, _vp, _vp, _vp]),
+    "rbfb_lbm_macros": (_i, [_i, _i, _vp, _vp, _vp, _vp, _vp]),
+    "rbfb_lbm_bgk": (_i, [_i, _i, _d, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "rbfb_lbm_stream_collide": (_i, [_i, _i, _i, _vp, _vp, _d, _vp, _vp, _vp, _vp, _vp, _vp]),
     "rbfb_autotune": (_i, [_vp, C.POINTER(Desc), _i, _vp, _vp, _i, _vp, _vp]),
     "rbfb_variant_name": (C.c_char_p, [_i]),
     "rbfb_select_variant": (_i, [_vp, C.POINTER(Desc), _i, _i, _i]),
@@ -468,6 +472,66 @@ def store_to_csr_stencil(nstencils, ia, va, W, ldw, idx, stream=None):
                                          _stream(stream))
     if st != OK:
         raise RbfError(st, "store_to_csr_stencil")
+
+
+# ---- D2Q9 lattice Boltzmann (src/lbm/d2q9_kernels.cu) ----------------------
+LBM_FP64, LBM_FP32 = 0, 1
+# lattice velocities c_a, a = 0..8: rest, E, N, W, S, NE, NW, SW, SE
+LBM_C = ((0, 0), (1, 0), (0, 1), (-1, 0), (0, -1), (1, 1), (-1, 1), (-1, -1), (1, -1))
+
+
+def _lbm_prec(t):
+    import torch
+    if t.dtype == torch.float64:
+        return LBM_FP64
+    if t.dtype == torch.float32:
+        return LBM_FP32
+    raise TypeError("LBM arrays are float32 or float64")
+
+
+def lbm_feq(rho, ux, uy, pdf, stream=None):
+    """pdf (9n) <- equilibrium populations of rho, ux, uy: feq_kernel."""
+    st = lib().rbfb_lbm_feq(rho.numel(), _lbm_prec(rho), _ptr(rho), _ptr(ux), _ptr(uy),
+                            _ptr(pdf), _stream(stream))
+    if st != OK:
+        raise RbfError(st, "lbm_feq")
+
+
+def lbm_macros(pdf, rho, ux, uy, stream=None):
+    """rho, ux, uy <- moments of pdf: macros_kernel."""
+    st = lib().rbfb_lbm_macros(rho.numel(), _lbm_prec(rho), _ptr(pdf), _ptr(rho), _ptr(ux),
+                               _ptr(uy), _stream(stream))
+    if st != OK:
+        raise RbfError(st, "lbm_macros")
+
+
+def lbm_bgk(omega, pdf, rho, ux, uy, indp=None, stream=None):
+    """BGK collision in place (bgk_kernel; bgk_kernel_split with indp)."""
+    st = lib().rbfb_lbm_bgk(rho.numel(), _lbm_prec(rho), float(omega), _ptr(pdf), _ptr(rho),
+                            _ptr(ux), _ptr(uy), _ptr(indp), _stream(stream))
+    if st != OK:
+        raise RbfError(st, "lbm_bgk")
+
+
+def lbm_stream_collide(k, ja, W, omega, pdf_in, pdf_out, rho=None, ux=None, uy=None,
+                       stream=None):
+    """One semi-Lagrangian step: stream pdf_in through the interpolation
+    operators W (8*n*k float64, direction a at [(a-1)*n*k:]) and collide into
+    pdf_out."""
+    n = pdf_in.numel() // 9
+    st = lib().rbfb_lbm_stream_collide(n, _lbm_prec(pdf_in), k, _ptr(ja), _ptr(W), float(omega),
+                                       _ptr(pdf_in), _ptr(pdf_out), _ptr(rho), _ptr(ux),
+                                       _ptr(uy), _stream(stream))
+    if st != OK:
+        raise RbfError(st, "lbm_stream_collide")
+
+
+def lbm_departure_points(dt):
+    """The 8 departure points -c_a dt (a = 1..8) in a stencil's local frame:
+    the interpolation points of the streaming operators."""
+    xc = np.array([-c[0] * dt for c in LBM_C[1:]], np.float64)
+    yc = np.array([-c[1] * dt for c in LBM_C[1:]], np.float64)
+    return xc, yc
 
 
 def solve_dp(A, ipiv, B, info, stream=None):

@@ -299,6 +299,41 @@ int rbfb_solve_bicgstab(rbfb_ctx* ctx, int n, int k, const int* ia, const int* j
                         double* u, double tol, int maxit, int* iters_h, double* relres_h,
                         void* stream);
 
+/* ---- D2Q9 lattice Boltzmann kernels that consume the operators -----------
+ * The reference's feq_kernel, macros_kernel, bgk_kernel and bgk_kernel_split
+ * (src/lbm/d2q9_kernels.cu:13-150, twins of src/lbm/d2q9_kernels.cuf:55-257),
+ * one thread per node, for float (RBFB_LBM_FP32) and double (RBFB_LBM_FP64)
+ * arrays. Lattice directions: 0 rest; 1-4 E, N, W, S; 5-8 NE, NW, SW, SE.
+ * Storage is planar: direction a of node i at pdf[i + n*a]. Each product,
+ * sum and quotient of the reference's expressions is rounded once, in its
+ * order (no fused multiply-adds). Asynchronous on `stream`. */
+#define RBFB_LBM_FP64 0
+#define RBFB_LBM_FP32 1
+/* pdf <- the equilibrium populations of (rho, ux, uy): feq_kernel. */
+int rbfb_lbm_feq(int n, int precision, const void* rho, const void* ux, const void* uy, void* pdf,
+                 void* stream);
+/* rho, ux, uy <- the moments of pdf: macros_kernel. */
+int rbfb_lbm_macros(int n, int precision, const void* pdf, void* rho, void* ux, void* uy,
+                    void* stream);
+/* BGK collision of pdf in place with relaxation rate omega; rho, ux, uy of
+ * the pre-collision populations: bgk_kernel, or bgk_kernel_split when indp
+ * (the direction-independent part of the equilibrium) is not NULL. */
+int rbfb_lbm_bgk(int n, int precision, double omega, void* pdf, void* rho, void* ux, void* uy,
+                 void* indp, void* stream);
+/* One semi-Lagrangian time step: streaming of the post-collision field
+ * pdf_in through the interpolation operators, then the BGK collision, into
+ * pdf_out (must not alias pdf_in). Direction a (1..8) of node s becomes
+ * sum_j W[(a-1)*n*k + s*k + j] * pdf_in[ja[s*k + j] + n*a] -- the weights of
+ * interpolation at the departure point x_s - c_a dt, as rbfb_assemble
+ * returns them for RBFB_OP_INTERP at those 8 points (W: 8 consecutive arrays
+ * of n*k doubles, FP64; rounded to float for RBFB_LBM_FP32); the rest
+ * population stays. rho, ux, uy (each may be NULL) receive the moments of
+ * the streamed populations. k <= 64. The reference assembles these
+ * operators (src/rbf_operators.h:292-298) but ships no streaming kernel. */
+int rbfb_lbm_stream_collide(int n, int precision, int k, const int* ja, const double* W,
+                            double omega, const void* pdf_in, void* pdf_out, void* rho, void* ux,
+                            void* uy, void* stream);
+
 /* ---- node renumbering (locality) ------------------------------------------
  * A permutation is stored in gather form, as the reference's
  * rbf::Permutation (src/rbf_reorder.h:68-80): perm[i] is the OLD index of

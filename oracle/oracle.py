@@ -24,12 +24,14 @@ HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "_build" / "liboracle.so"
 REF_SO = HERE / "_ref" / "libref_knn.so"
 REF_FILL_SO = HERE / "_ref" / "libref_fill.so"
+REF_LBM_SO = HERE / "_ref" / "libref_lbm.so"
 
 OP_INTERP, OP_LAPLACE, OP_DX, OP_DY, OP_DXX, OP_DYY, OP_DXY = 1, 2, 4, 8, 16, 32, 64
 
 _lib = None
 _ref = None
 _ref_fill = None
+_ref_lbm = None
 
 _dp = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
@@ -93,6 +95,14 @@ def lib():
         L.orc_system.argtypes = [C.c_int, _dp, _dp, C.c_int, _ip, C.c_int, C.c_int, C.c_int,
                                  C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_double, C.c_double,
                                  _dp, _dp, _dp]
+        for nm in ("orc_lbm_feq", "orc_lbm_macros", "orc_lbm_bgk", "orc_lbm_stream_collide"):
+            getattr(L, nm).restype = None
+        L.orc_lbm_feq.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 4
+        L.orc_lbm_macros.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 4
+        L.orc_lbm_bgk.argtypes = [C.c_int, C.c_int, C.c_double] + [C.c_void_p] * 5
+        L.orc_lbm_stream_collide.argtypes = [C.c_int, C.c_int, C.c_int, _ip, _dp, C.c_double,
+                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_void_p]
         L.orc_phs.restype = C.c_double
         L.orc_phs.argtypes = [C.c_int, C.c_double]
         L.orc_set_threads.argtypes = [C.c_int]
@@ -173,6 +183,65 @@ def system(s, x, y, idx, P, Q=None, ops=OP_LAPLACE | OP_DX | OP_DY, xc=None, yc=
     if e == -1000:
         raise ValueError("oracle rejected the arguments")
     return xs, ys, a.reshape(n, n + nrhs), e
+
+
+def _lbm_p(a):
+    return 0 if a.dtype == np.float64 else 1
+
+
+def lbm_feq(rho, ux, uy):
+    """feq_kernel restated: the 9 x n planar equilibrium populations."""
+    pdf = np.empty(9 * rho.size, rho.dtype)
+    lib().orc_lbm_feq(rho.size, _lbm_p(rho), rho.ctypes.data, ux.ctypes.data, uy.ctypes.data,
+                      pdf.ctypes.data)
+    return pdf
+
+
+def lbm_macros(pdf):
+    """macros_kernel restated: (rho, ux, uy) of planar populations."""
+    n = pdf.size // 9
+    rho, ux, uy = (np.empty(n, pdf.dtype) for _ in range(3))
+    lib().orc_lbm_macros(n, _lbm_p(pdf), pdf.ctypes.data, rho.ctypes.data, ux.ctypes.data,
+                         uy.ctypes.data)
+    return rho, ux, uy
+
+
+def lbm_bgk(pdf, omega):
+    """bgk_kernel_split restated on a copy: (pdf, rho, ux, uy, indp)."""
+    pdf = np.array(pdf, copy=True)
+    n = pdf.size // 9
+    rho, ux, uy, indp = (np.empty(n, pdf.dtype) for _ in range(4))
+    lib().orc_lbm_bgk(n, _lbm_p(pdf), float(omega), pdf.ctypes.data, rho.ctypes.data,
+                      ux.ctypes.data, uy.ctypes.data, indp.ctypes.data)
+    return pdf, rho, ux, uy, indp
+
+
+def lbm_stream_collide(k, ja, W, omega, pdf):
+    """One streaming + collision step restated: (pdf_out, rho, ux, uy)."""
+    n = pdf.size // 9
+    out = np.empty_like(pdf)
+    rho, ux, uy = (np.empty(n, pdf.dtype) for _ in range(3))
+    lib().orc_lbm_stream_collide(n, _lbm_p(pdf), k, _i32(ja), _f64(W), float(omega),
+                                 pdf.ctypes.data, out.ctypes.data, rho.ctypes.data,
+                                 ux.ctypes.data, uy.ctypes.data)
+    return out, rho, ux, uy
+
+
+def ref_lbm_lib():
+    """The reference's own D2Q9 kernels (GPU; launchers take device
+    pointers), or None when not built here."""
+    global _ref_lbm
+    if _ref_lbm is None:
+        if not REF_LBM_SO.exists():
+            return None
+        L = C.CDLL(str(REF_LBM_SO))
+        L.ref_lbm_feq.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 4
+        L.ref_lbm_macros.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 4
+        L.ref_lbm_bgk_split.argtypes = [C.c_int, C.c_int, C.c_double] + [C.c_void_p] * 5
+        for nm in ("ref_lbm_feq", "ref_lbm_macros", "ref_lbm_bgk_split"):
+            getattr(L, nm).restype = C.c_int
+        _ref_lbm = L
+    return _ref_lbm
 
 
 def set_threads(n: int) -> None:

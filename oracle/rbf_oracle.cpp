@@ -964,3 +964,205 @@ extern "C" int orc_bicgstab(int n, int k, const int* ia, const int* ja, const do
         rho = rho_new;
     }
 }
+
+// ---- D2Q9 lattice Boltzmann -------------------------------------------------
+//
+// Restates feq_kernel, macros_kernel and bgk_kernel_split of the reference
+// (src/lbm/d2q9_kernels.cu:13-150; lattice constants src/lbm/d2q9_kernels.h:
+// 16-31) for float and double: every product, sum and quotient in the
+// source's order, each rounded once (this file is compiled with
+// -ffp-contract=off). Planar storage, direction a of node i at pdf[i + n*a].
+// The streaming step (which the reference does not ship) sums the
+// interpolation weights times the gathered populations in the order the CUDA
+// kernel does: lane j of a warp forms w_j * f_j (j < k) and adds w_{j+32} *
+// f_{j+32} with a fused multiply-add (j + 32 < k); an xor butterfly over 32
+// lanes (offsets 16, 8, 4, 2, 1) adds the lanes.
+namespace lbm {
+
+template <typename T>
+struct Lat {
+    static constexpr T w0 = T(4) / T(9);
+    static constexpr T ws = T(1) / T(9);
+    static constexpr T wd = T(1) / T(36);
+    static constexpr T three_w0 = T(3) * w0;
+    static constexpr T three_ws = T(3) * ws;
+    static constexpr T three_wd = T(3) * wd;
+    static constexpr T one_third = T(1) / T(3);
+    static constexpr T one_half = T(1) / T(2);
+    static constexpr T three_halves = T(3) / T(2);
+};
+
+template <typename T>
+void moments(const T* f, T& rho, T& ux, T& uy) {
+    rho = (((f[5] + f[7]) + (f[6] + f[8])) + ((f[1] + f[3]) + (f[2] + f[4]))) + f[0];
+    const T invrho = T(1) / rho;
+    ux = invrho * (((f[5] - f[7]) + (f[8] - f[6])) + (f[1] - f[3]));
+    uy = invrho * (((f[5] - f[7]) + (f[6] - f[8])) + (f[2] - f[4]));
+}
+
+// out[a] = s_a * rho * term_a + omegabar * f[a] (omegabar * f absent when
+// f == nullptr: the equilibrium itself, feq_kernel's form)
+template <typename T>
+void relax(const T* f, T omegabar, T s0, T ss, T sd, T rho, T ux, T uy, T* out, T* indp_out) {
+    using L = Lat<T>;
+    const T uxsq = ux * ux;
+    const T uysq = uy * uy;
+    const T indp = L::one_third - L::one_half * (uxsq + uysq);
+    if (indp_out) *indp_out = indp;
+    T term[9];
+    term[0] = indp;
+    const T v13 = indp + L::three_halves * uxsq;
+    term[1] = v13 + ux;
+    term[3] = v13 - ux;
+    const T v24 = indp + L::three_halves * uysq;
+    term[2] = v24 + uy;
+    term[4] = v24 - uy;
+    const T xpy = ux + uy;
+    const T v57 = indp + L::three_halves * xpy * xpy;
+    term[5] = v57 + xpy;
+    term[7] = v57 - xpy;
+    const T xmy = ux - uy;
+    const T v68 = indp + L::three_halves * xmy * xmy;
+    term[6] = v68 - xmy;
+    term[8] = v68 + xmy;
+    const T sc[9] = {s0, ss, ss, ss, ss, sd, sd, sd, sd};
+    for (int a = 0; a < 9; ++a) {
+        const T e = sc[a] * rho * term[a];
+        out[a] = f ? omegabar * f[a] + e : e;
+    }
+}
+
+template <typename T>
+void feq(int n, const T* rho, const T* ux, const T* uy, T* pdf) {
+    using L = Lat<T>;
+    const size_t N = static_cast<size_t>(n);
+    for (int i = 0; i < n; ++i) {
+        T out[9];
+        relax<T>(nullptr, T(0), L::three_w0, L::three_ws, L::three_wd, rho[i], ux[i], uy[i], out,
+                 nullptr);
+        for (int a = 0; a < 9; ++a) pdf[i + N * a] = out[a];
+    }
+}
+
+template <typename T>
+void collide(const T* f, T omega, T* out, T* rho, T* ux, T* uy, T* indp) {
+    using L = Lat<T>;
+    const T omegabar = T(1) - omega;
+    moments(f, *rho, *ux, *uy);
+    relax<T>(f, omegabar, omega * L::three_w0, omega * L::three_ws, omega * L::three_wd, *rho,
+             *ux, *uy, out, indp);
+}
+
+template <typename T>
+void bgk(int n, T omega, T* pdf, T* rho, T* ux, T* uy, T* indp) {
+    const size_t N = static_cast<size_t>(n);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; ++i) {
+        T f[9], o[9], d;
+        for (int a = 0; a < 9; ++a) f[a] = pdf[i + N * a];
+        collide(f, omega, o, rho + i, ux + i, uy + i, &d);
+        if (indp) indp[i] = d;
+        for (int a = 0; a < 9; ++a) pdf[i + N * a] = o[a];
+    }
+}
+
+template <typename T>
+void macros(int n, const T* pdf, T* rho, T* ux, T* uy) {
+    const size_t N = static_cast<size_t>(n);
+    for (int i = 0; i < n; ++i) {
+        T f[9];
+        for (int a = 0; a < 9; ++a) f[a] = pdf[i + N * a];
+        moments(f, rho[i], ux[i], uy[i]);
+    }
+}
+
+template <typename T>
+T fma_t(T a, T b, T c) {
+    return std::fma(a, b, c);
+}
+
+template <typename T>
+void stream_collide(int n, int k, const int* ja, const double* W, T omega, const T* pin, T* pout,
+                    T* rho, T* ux, T* uy) {
+    const size_t N = static_cast<size_t>(n);
+    const size_t nnz = N * static_cast<size_t>(k);
+#pragma omp parallel for schedule(static)
+    for (int s = 0; s < n; ++s) {
+        const size_t row = static_cast<size_t>(s) * k;
+        T f[9];
+        f[0] = pin[s];
+        for (int a = 1; a < 9; ++a) {
+            const double* Wa = W + static_cast<size_t>(a - 1) * nnz + row;
+            T v[32];
+            for (int l = 0; l < 32; ++l) {
+                T t = T(0);
+                if (l < k) t = static_cast<T>(Wa[l]) * pin[ja[row + l] + N * a];
+                if (l + 32 < k) t = fma_t(static_cast<T>(Wa[l + 32]), pin[ja[row + l + 32] + N * a], t);
+                v[l] = t;
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                T w[32];
+                for (int l = 0; l < 32; ++l) w[l] = v[l] + v[l ^ o];
+                for (int l = 0; l < 32; ++l) v[l] = w[l];
+            }
+            f[a] = v[0];
+        }
+        T o[9], r, u, w, d;
+        collide(f, omega, o, &r, &u, &w, &d);
+        for (int a = 0; a < 9; ++a) pout[s + N * a] = o[a];
+        if (rho) rho[s] = r;
+        if (ux) ux[s] = u;
+        if (uy) uy[s] = w;
+    }
+}
+
+}  // namespace lbm
+
+extern "C" {
+
+// precision 0: double arrays, 1: float arrays (RBFB_LBM_FP64 / RBFB_LBM_FP32)
+void orc_lbm_feq(int n, int precision, const void* rho, const void* ux, const void* uy, void* pdf) {
+    if (precision == 0)
+        lbm::feq<double>(n, static_cast<const double*>(rho), static_cast<const double*>(ux),
+                         static_cast<const double*>(uy), static_cast<double*>(pdf));
+    else
+        lbm::feq<float>(n, static_cast<const float*>(rho), static_cast<const float*>(ux),
+                        static_cast<const float*>(uy), static_cast<float*>(pdf));
+}
+
+void orc_lbm_macros(int n, int precision, const void* pdf, void* rho, void* ux, void* uy) {
+    if (precision == 0)
+        lbm::macros<double>(n, static_cast<const double*>(pdf), static_cast<double*>(rho),
+                            static_cast<double*>(ux), static_cast<double*>(uy));
+    else
+        lbm::macros<float>(n, static_cast<const float*>(pdf), static_cast<float*>(rho),
+                           static_cast<float*>(ux), static_cast<float*>(uy));
+}
+
+void orc_lbm_bgk(int n, int precision, double omega, void* pdf, void* rho, void* ux, void* uy,
+                 void* indp) {
+    if (precision == 0)
+        lbm::bgk<double>(n, omega, static_cast<double*>(pdf), static_cast<double*>(rho),
+                         static_cast<double*>(ux), static_cast<double*>(uy),
+                         static_cast<double*>(indp));
+    else
+        lbm::bgk<float>(n, static_cast<float>(omega), static_cast<float*>(pdf),
+                        static_cast<float*>(rho), static_cast<float*>(ux), static_cast<float*>(uy),
+                        static_cast<float*>(indp));
+}
+
+void orc_lbm_stream_collide(int n, int precision, int k, const int* ja, const double* W,
+                            double omega, const void* pin, void* pout, void* rho, void* ux,
+                            void* uy) {
+    if (precision == 0)
+        lbm::stream_collide<double>(n, k, ja, W, omega, static_cast<const double*>(pin),
+                                    static_cast<double*>(pout), static_cast<double*>(rho),
+                                    static_cast<double*>(ux), static_cast<double*>(uy));
+    else
+        lbm::stream_collide<float>(n, k, ja, W, static_cast<float>(omega),
+                                   static_cast<const float*>(pin), static_cast<float*>(pout),
+                                   static_cast<float*>(rho), static_cast<float*>(ux),
+                                   static_cast<float*>(uy));
+}
+
+}  // extern "C"

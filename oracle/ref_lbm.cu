@@ -1,0 +1,69 @@
+// ref_lbm.cu -- host launchers for the reference's own D2Q9 kernels
+// (feq_kernel, macros_kernel, bgk_kernel_split: src/lbm/d2q9_kernels.cu and
+// its header), for both instantiations.
+//
+// TEST INFRASTRUCTURE. oracle/Makefile compiles this file together with the
+// reference's d2q9_kernels.cu where it lies (nothing of it is copied here)
+// into oracle/_ref/libref_lbm.so, with --fmad=false so that every product and
+// sum is rounded as the source writes it. Only the GPU tests load it: it pins
+// the library's LBM kernels to the reference's own, bit for bit. The
+// launchers take device pointers and synchronise; they allocate nothing.
+#include <cuda_runtime.h>
+
+#include "d2q9_kernels.h"
+
+namespace {
+inline int grid(int n) { return (n + 255) / 256; }
+inline int done() { return cudaDeviceSynchronize() == cudaSuccess ? 0 : -1; }
+}  // namespace
+
+extern "C" {
+
+// precision 0: double arrays, 1: float arrays
+int ref_lbm_feq(int n, int precision, const void* rho, const void* ux, const void* uy, void* pdf) {
+    if (n <= 0) return 0;
+    if (precision == 0)
+        feq_kernel<double><<<grid(n), 256>>>(n, static_cast<const double*>(rho),
+                                             static_cast<const double*>(ux),
+                                             static_cast<const double*>(uy),
+                                             static_cast<double*>(pdf));
+    else
+        feq_kernel<float><<<grid(n), 256>>>(n, static_cast<const float*>(rho),
+                                            static_cast<const float*>(ux),
+                                            static_cast<const float*>(uy), static_cast<float*>(pdf));
+    return done();
+}
+
+int ref_lbm_macros(int n, int precision, const void* pdf, void* rho, void* ux, void* uy) {
+    if (n <= 0) return 0;
+    if (precision == 0)
+        macros_kernel<double><<<grid(n), 256>>>(n, static_cast<const double*>(pdf),
+                                                static_cast<double*>(rho),
+                                                static_cast<double*>(ux),
+                                                static_cast<double*>(uy));
+    else
+        macros_kernel<float><<<grid(n), 256>>>(n, static_cast<const float*>(pdf),
+                                               static_cast<float*>(rho), static_cast<float*>(ux),
+                                               static_cast<float*>(uy));
+    return done();
+}
+
+int ref_lbm_bgk_split(int n, int precision, double omega, void* pdf, void* rho, void* ux, void* uy,
+                      void* indp) {
+    if (n <= 0) return 0;
+    if (precision == 0)
+        bgk_kernel_split<double><<<grid(n), 256>>>(n, omega, static_cast<double*>(pdf),
+                                                   static_cast<double*>(rho),
+                                                   static_cast<double*>(ux),
+                                                   static_cast<double*>(uy),
+                                                   static_cast<double*>(indp));
+    else
+        bgk_kernel_split<float><<<grid(n), 256>>>(n, static_cast<float>(omega),
+                                                  static_cast<float*>(pdf),
+                                                  static_cast<float*>(rho),
+                                                  static_cast<float*>(ux), static_cast<float*>(uy),
+                                                  static_cast<float*>(indp));
+    return done();
+}
+
+}  // extern "C"
