@@ -24,7 +24,10 @@ set) and, at N = 1, the other configurations:
       FP64 and mixed, errors against the long-double oracle, fallbacks;
   c5  the 2,000-request serving stream under a 40 GB HBM budget: p50/p99
       latency at 80 % of the measured capacity over repeats (with spread),
-      aggregate stencils/s against serial plain FP64.
+      aggregate stencils/s against serial plain FP64;
+  lbm the D2Q9 lattice Boltzmann step that consumes interpolation operators
+      (fused semi-Lagrangian streaming + BGK collision) on the 1024^2 grid,
+      with its HBM roofline fraction.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -387,6 +390,69 @@ def config4(R, O, NS, torch, ctx, dev, reps=3):
     return res
 
 
+def lbm_bytes_per_node(k):
+    """Compulsory HBM bytes of one stream + collide step per node: its ja row
+    (4k), its 8 weight rows (64k), its 9 populations read and written, and
+    rho, ux, uy written (the gathered neighbour populations are the same
+    arrays again: L2 reuse)."""
+    return 4 * k + 64 * k + 9 * 8 + 9 * 8 + 3 * 8
+
+
+def config_lbm(R, NS, torch, ctx, dev, m=M_GRID, k=21, steps=20):
+    """D2Q9 semi-Lagrangian lattice Boltzmann on the periodic m x m grid:
+    interpolation operators at the 8 departure points (k = 21, r^3 +
+    degree 2, dt = h/2) assembled once, then fused stream + collide steps
+    (FP64), timed with CUDA events."""
+    x, y, _ = NS.jittered_grid(m, 0.3, seed=2, periodic=True)
+    n = x.size
+    xd, yd = torch.as_tensor(x, device=dev), torch.as_tensor(y, device=dev)
+    ja = torch.empty(n * k, dtype=torch.int32, device=dev)
+    ctx.knn_stencils(xd, yd, k, ja, period=(1.0, 1.0))
+    xc, yc = R.lbm_departure_points(0.5 / m)
+    xcd, ycd = torch.as_tensor(xc, device=dev), torch.as_tensor(yc, device=dev)
+    W = torch.empty(8 * n * k, dtype=torch.float64, device=dev)
+    vals = [W[a * n * k:(a + 1) * n * k] for a in range(8)]
+    d = R.make_desc(2, 3, R.OP_INTERP, R.FP64, True, period=(1.0, 1.0), xc=xcd, yc=ycd, nc=8)
+    st = ctx.assemble(d, xd, yd, k, ja, vals, stats=True)
+    rho = 1.0 + 0.02 * np.sin(2 * np.pi * x)
+    ux = 0.03 * np.cos(2 * np.pi * y)
+    uy = 0.01 * np.sin(2 * np.pi * (x + y))
+    fa = torch.empty(9 * n, dtype=torch.float64, device=dev)
+    R.lbm_feq(torch.as_tensor(rho, device=dev), torch.as_tensor(ux, device=dev),
+              torch.as_tensor(uy, device=dev), fa)
+    fb = torch.empty_like(fa)
+    r, u, v = (torch.empty(n, dtype=torch.float64, device=dev) for _ in range(3))
+    stream = torch.cuda.current_stream(dev)
+    bufs = [fa, fb]
+
+    def one(i):
+        R.lbm_stream_collide(k, ja, W, 1.5, bufs[i % 2], bufs[(i + 1) % 2], r, u, v,
+                             stream=stream)
+    for i in range(3):
+        one(i)
+    torch.cuda.synchronize()
+    ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ea.record(stream)
+    for i in range(steps):
+        one(i)
+    eb.record(stream)
+    torch.cuda.synchronize()
+    ms = ea.elapsed_time(eb) / steps
+    pk, src = peaks()
+    gbs = lbm_bytes_per_node(k) * n / (ms * 1e-3) / 1e9
+    out = {"workload": f"D2Q9 semi-Lagrangian LBM, periodic {m}x{m} jittered grid, k={k} "
+                       "interpolation operators (r^3 + degree 2) at the 8 departure points "
+                       "x - c_a h/2, FP64, fused stream + BGK collide per step",
+           "nodes": n, "ms_per_step": ms, "node_updates_per_s": n / (ms * 1e-3),
+           "operator_assembly_ms": st["ms"],
+           "hbm": {"bytes_per_node": lbm_bytes_per_node(k), "achieved_gbs": gbs,
+                   "peak_gbs": pk.get("hbm_gbs"), "frac": gbs / pk.get("hbm_gbs"),
+                   "peak_source": src}}
+    del W, vals, fa, fb, ja
+    torch.cuda.synchronize()
+    return out
+
+
 def serve_sample(R, NS, device, count, form="fp64", repeats=3):
     """The serving configuration: `count` requests (sizes log-uniform in
     [1e3, 5e5], square or disk, k in {21, 35, 64} with degree {2, 3, 4})
@@ -424,7 +490,7 @@ def serve_sample(R, NS, device, count, form="fp64", repeats=3):
             if st != 0 or res.status != 0:
                 raise RuntimeError(f"serving request failed: {st} {res.status}")
             lat.append(res.end_ms - res.submit_ms)
-            win.append((res.start_ms, res.end_ms))
+            win.append((res.dev_start_ms, res.dev_end_ms))
             srv.release(t)
             del pending[t]
 
@@ -678,7 +744,8 @@ def main():
     if ws == 1 and not args.no_configs:
         del vals, ja, info
         torch.cuda.synchronize()
-        configs = {"c3": config3(R, O, torch, ctx, dev), "c4": config4(R, O, NS, torch, ctx, dev)}
+        configs = {"c3": config3(R, O, torch, ctx, dev), "c4": config4(R, O, NS, torch, ctx, dev),
+                   "lbm": config_lbm(R, NS, torch, ctx, dev)}
         if args.serve_requests > 0:
             configs["c5"] = serve_sample(R, NS, local, args.serve_requests,
                                          "fp64" if d_head is d_f64 else "mixed",

@@ -51,14 +51,14 @@
 
 namespace rbfb {
 
-template <typename T, int NMAX, int NRHS, int P, int Q, bool MIXED, int PB>
-struct BlkCfg {
+// Layout of one stencil's working set for systems of up to NMAX unknowns
+// with up to KMAX neighbours (shared memory, or a global scratch region).
+template <typename T, int NMAX, int NRHS, int KMAX_, int PB>
+struct BlkLayout {
     static constexpr int G = 32;  // lanes per stencil: one warp
-    static constexpr int NP = npoly(P);
-    static constexpr int KMAX = NMAX - NP;
+    static constexpr int KMAX = KMAX_;
     static constexpr int R = (NMAX + G - 1) / G;  // list positions per lane
     static constexpr int VE = 16 / (int)sizeof(T);  // elements per 16-byte vector
-    static_assert(!MIXED, "the blocked kernel is FP64");
     static_assert(PB % VE == 0, "panels are whole vectors");
     static_assert(NMAX <= 128, "pivot keys carry the list position in 7 bits");
     static constexpr int WMAX = NMAX + NRHS;  // columns: unknowns + right-hand sides
@@ -83,6 +83,12 @@ struct BlkCfg {
     static constexpr int off_nxy = off_nja + al16(4 * KMAX);
     static constexpr int off_nia = off_nxy + 16;
     static constexpr int bytes = off_nia + 16;
+};
+
+template <typename T, int NMAX, int NRHS, int P, int Q, bool MIXED, int PB>
+struct BlkCfg : BlkLayout<T, NMAX, NRHS, NMAX - npoly(P), PB> {
+    static_assert(!MIXED, "the blocked kernel is FP64");
+    static constexpr int NP = npoly(P);
 };
 
 // 16-byte vector moves between shared memory and register arrays.
@@ -112,99 +118,66 @@ __device__ __forceinline__ uint32_t hiword(double v) {
 }
 __device__ __forceinline__ uint32_t hiword(float v) { return __float_as_uint(v); }
 
-template <typename T, int NMAX, int NRHS, int P, int Q, bool MIXED, int PB, bool PF>
-__device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, char* smem,
-                                             int lane) {
-    using C = BlkCfg<T, NMAX, NRHS, P, Q, MIXED, PB>;
-    constexpr int G = C::G, NP = C::NP, R = C::R, VE = C::VE, LDS = C::LDS;
-    constexpr unsigned FULL = 0xffffffffu;
-    double* cx = reinterpret_cast<double*>(smem + C::off_cx);
-    double* cy = reinterpret_cast<double*>(smem + C::off_cy);
-    T* S = reinterpret_cast<T*>(smem + C::off_s);
-    T* X = reinterpret_cast<T*>(smem + C::off_x);
-    T* pinv = reinterpret_cast<T*>(smem + C::off_pinv);
-    int* piv = reinterpret_cast<int*>(smem + C::off_piv);
-    int* act = reinterpret_cast<int*>(smem + C::off_act);
-    unsigned char* alive = reinterpret_cast<unsigned char*>(smem + C::off_alive);
-    int* nja = reinterpret_cast<int*>(smem + C::off_nja);
-    double* nxy = reinterpret_cast<double*>(smem + C::off_nxy);
-    int* nia = reinterpret_cast<int*>(smem + C::off_nia);
+// ---- the phases of one stencil, shared by the fixed-shape and the uneven
+// kernels. A stencil's working set (S, X, pinv, piv, act, alive, cx, cy) is
+// in shared memory, or -- for the uneven kernel's large stencils -- in a
+// global scratch region of the same layout.
 
-    // With PF, stencil s was prefetched (by the previous call of this warp, or
-    // by prefetch_first): its neighbour coordinates wait in cx/cy (raw), its
-    // centre in nxy, its CSR bounds in nia. Without PF everything comes from
-    // global memory.
-    int off, ks;
-    double x0, y0;
-    if constexpr (PF) {
-        cp_async_wait_all();
-        __syncwarp();
-        x0 = nxy[0];
-        y0 = nxy[1];
-        off = p.ia ? nia[0] : (s - p.row_base) * p.k;
-        ks = p.ia ? nia[1] - off : p.k;
-        __syncwarp();  // read before the slots are refilled below
-    } else {
-        x0 = p.x[s];
-        y0 = p.y[s];
-        off = p.ia ? p.ia[s] : (s - p.row_base) * p.k;
-        ks = p.ia ? p.ia[s + 1] - off : p.k;
-    }
-    const int n = NP + ks;
-    const int W = n + NRHS;  // columns in use
-    if (PF && sn >= 0 && lane == 0) {  // prefetch stage 1: next centre and CSR bounds
-        cp_async8(nxy, p.x + sn);
-        cp_async8(nxy + 1, p.y + sn);
-        if (p.ia) {
-            cp_async4(nia, p.ia + sn);
-            cp_async4(nia + 1, p.ia + sn + 1);
+// Gather + FP64 shift to the centre (x0, y0) (+ minimum image), and the
+// power-of-two radius scale (src/rbf_operators.h:354-358): cx/cy receive the
+// shifted, scaled coordinates of the ks neighbours (with PF they hold the
+// raw prefetched ones on entry). Returns the scale exponent e.
+template <int KMAX, bool PF>
+__device__ __forceinline__ int gather_scale(const AsmParams& p, int off, int ks, double x0,
+                                            double y0, double* cx, double* cy, int lane) {
+    constexpr int G = 32, KPL = (KMAX + G - 1) / G;
+    double gx[KPL], gy[KPL];
+    int emax = -100000;
+#pragma unroll
+    for (int t = 0; t < KPL; ++t) {
+        const int j = lane + t * G;
+        gx[t] = 0.0;
+        gy[t] = 0.0;
+        if (j < ks) {
+            double xn, yn;
+            if constexpr (PF) {
+                xn = cx[j];
+                yn = cy[j];
+            } else {
+                const int nb = __ldg(p.ja + off + j);
+                xn = __ldg(p.x + nb);
+                yn = __ldg(p.y + nb);
+            }
+            gx[t] = min_image(dsub(xn, x0), p.Lx);
+            gy[t] = min_image(dsub(yn, y0), p.Ly);
+            if (gx[t] != 0.0) emax = max(emax, ilogb(fabs(gx[t])) + 1);
+            if (gy[t] != 0.0) emax = max(emax, ilogb(fabs(gy[t])) + 1);
         }
     }
-
-    // ---- gather + FP64 shift (+ minimum image), src/rbf_operators.h:354-358,
-    // and the power-of-two radius scale
-    int e;
-    {
-        constexpr int KPL = (C::KMAX + G - 1) / G;
-        double gx[KPL], gy[KPL];
-        int emax = -100000;
+    int e = __reduce_max_sync(0xffffffffu, emax);
+    e = (p.scale && e > -100000) ? e : 0;
 #pragma unroll
-        for (int t = 0; t < KPL; ++t) {
-            const int j = lane + t * G;
-            gx[t] = 0.0;
-            gy[t] = 0.0;
-            if (j < ks) {
-                double xn, yn;
-                if constexpr (PF) {
-                    xn = cx[j];
-                    yn = cy[j];
-                } else {
-                    const int nb = __ldg(p.ja + off + j);
-                    xn = __ldg(p.x + nb);
-                    yn = __ldg(p.y + nb);
-                }
-                gx[t] = min_image(dsub(xn, x0), p.Lx);
-                gy[t] = min_image(dsub(yn, y0), p.Ly);
-                if (gx[t] != 0.0) emax = max(emax, ilogb(fabs(gx[t])) + 1);
-                if (gy[t] != 0.0) emax = max(emax, ilogb(fabs(gy[t])) + 1);
-            }
-        }
-        e = __reduce_max_sync(FULL, emax);
-        e = (p.scale && e > -100000) ? e : 0;
-#pragma unroll
-        for (int t = 0; t < KPL; ++t) {
-            const int j = lane + t * G;
-            if (j < ks) {
-                cx[j] = scalbn(gx[t], -e);
-                cy[j] = scalbn(gy[t], -e);
-            }
+    for (int t = 0; t < KPL; ++t) {
+        const int j = lane + t * G;
+        if (j < ks) {
+            cx[j] = scalbn(gx[t], -e);
+            cy[j] = scalbn(gy[t], -e);
         }
     }
     __syncwarp();
+    return e;
+}
 
-    // ---- fill S: phi block (each unordered pair once, a flat walk over the
-    // lanes), monomial rows and columns, zero polynomial block, right-hand
-    // sides (fill_matrix / fill_rhs, src/rbf_operators.h:116-185)
+// The augmented system in S (row stride LDS): phi block (each unordered pair
+// once, a flat walk over the lanes), monomial rows and columns, zero
+// polynomial block, right-hand sides as columns n .. n+NRHS-1 (fill_matrix /
+// fill_rhs, src/rbf_operators.h:116-185); alive[r] = r < n for r < nmax.
+template <typename T, int LDS, int NRHS, int P, int Q>
+__device__ __forceinline__ void fill_system(const AsmParams& p, T* S, const double* cx,
+                                            const double* cy, int ks, int e,
+                                            unsigned char* alive, int nmax, int lane) {
+    constexpr int G = 32, NP = npoly(P);
+    const int n = NP + ks;
     {
         const int npair = ks * (ks - 1) / 2;
         int i = 0, j = 1 + lane;
@@ -246,29 +219,18 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
         for (int q = 0; q < NRHS; ++q)
             S[r * LDS + n + q] = static_cast<T>(q < p.nrhs ? rhs_poly<P>(p, q, r, e) : 0.0);
     }
-    for (int r = lane; r < NMAX; r += G) alive[r] = r < n ? 1 : 0;
+    for (int r = lane; r < nmax; r += G) alive[r] = r < n ? 1 : 0;
+}
 
-    // prefetch stage 2: the next stencil's ja row (its bounds have landed)
-    if constexpr (PF) {
-        int offn = 0, ksn = 0;
-        if (sn >= 0) {
-            if (p.ia) {
-                cp_async_wait_all();
-                __syncwarp();
-                offn = nia[0];
-                ksn = nia[1] - offn;
-            } else {
-                offn = (sn - p.row_base) * p.k;
-                ksn = p.k;
-            }
-            for (int j = lane; j < ksn; j += G) cp_async4(nja + j, p.ja + offn + j);
-        }
-        __syncwarp();
-        if (lane == 0) nia[2] = ksn;
-    }
-    __syncwarp();
-
-    // ---- blocked elimination
+// Blocked right-looking elimination of the n x n system in S with its NRHS
+// right-hand-side columns (panels of PB; R list positions per lane, R*32 >=
+// n). Returns info: 0, or c + 1 for the first zero pivot.
+template <typename T, int R, int LDS, int NRHS, int PB>
+__device__ __forceinline__ int eliminate_blocked(T* S, T* pinv, int* piv, int* act,
+                                                 unsigned char* alive, int n, int lane) {
+    constexpr int G = 32, VE = 16 / (int)sizeof(T);
+    constexpr unsigned FULL = 0xffffffffu;
+    const int W = n + NRHS;  // columns in use
     int info = 0;
 #pragma unroll 1
     for (int c0 = 0; c0 < n; c0 += PB) {
@@ -277,7 +239,7 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
 #pragma unroll
         for (int j = 0; j < R; ++j) {
             const int r = lane + G * j;
-            const bool a = r < NMAX && alive[r];
+            const bool a = r < n && alive[r];
             const unsigned b = __ballot_sync(FULL, a);
             if (a) act[m + __popc(b & ((1u << lane) - 1u))] = r;
             m += __popc(b);
@@ -400,7 +362,7 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
         __syncwarp();
         // 5. the unused rows over the trailing columns (all lanes walk the same
         // columns: the pivot-row values are broadcast loads)
-        if (tend == PB) {
+        if (m > tend) {
             bool any[R];
 #pragma unroll
             for (int sl = 0; sl < R; ++sl) any[sl] = __any_sync(FULL, kmask[sl] != 0u);
@@ -427,9 +389,19 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
             __syncwarp();
         }
     }
+    return info;
+}
 
-    // ---- back substitution (column oriented): lane l holds the transformed
-    // right-hand sides of the rows pivoted at steps l, l + 32, ...
+// Column-oriented back substitution (the oracle's order): lane l holds the
+// transformed right-hand sides of the rows pivoted at steps l, l + 32, ...;
+// for c = n-1 .. 0 the owner of step c forms x_c = y * (1 / pivot_c) and
+// broadcasts it by shuffle, and the rows pivoted before c update with
+// u(row, c). X[c*NRHS + q] receives x_c.
+template <typename T, int R, int LDS, int NRHS>
+__device__ __forceinline__ void back_substitute_blk(const T* S, const T* pinv, const int* piv,
+                                                    T* X, int n, int lane) {
+    constexpr int G = 32;
+    constexpr unsigned FULL = 0xffffffffu;
     T y[R][NRHS];
     int prow_t[R];
 #pragma unroll
@@ -438,15 +410,6 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
         prow_t[sl] = t < n ? piv[t] : 0;
 #pragma unroll
         for (int q = 0; q < NRHS; ++q) y[sl][q] = t < n ? S[prow_t[sl] * LDS + n + q] : T(0);
-    }
-    // prefetch stage 3: the next stencil's neighbour coordinates into cx/cy
-    if (const int ksn = PF ? nia[2] : 0; ksn > 0) {
-        cp_async_wait_all();
-        for (int j = lane; j < ksn; j += G) {
-            const int nb = nja[j];
-            cp_async8(cx + j, p.x + nb);
-            cp_async8(cy + j, p.y + nb);
-        }
     }
 #pragma unroll 1
     for (int c = n - 1; c >= 0; --c) {
@@ -473,19 +436,108 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
         }
     }
     __syncwarp();
+}
 
-    // ---- scatter, src/rbf_operators.h:368-375
+// Scatter of the k node weights (unknowns NP .. NP+ks-1), rescaled,
+// src/rbf_operators.h:368-375; NaN for a singular stencil; info.
+template <typename T, int NRHS>
+__device__ __forceinline__ void scatter_blk(const AsmParams& p, const T* X, int np, int ks, int off,
+                                            int e, int info, int s, int lane) {
     const bool bad = info != 0;
     for (int q = 0; q < p.nrhs; ++q) {
         double* dst = out_column(p, q) + off;
         const int sh = -op_order(p.col_op[q]) * e;
-        for (int j = lane; j < ks; j += G) {
-            const double v = static_cast<double>(X[(NP + j) * NRHS + q]);
+        for (int j = lane; j < ks; j += 32) {
+            const double v = static_cast<double>(X[(np + j) * NRHS + q]);
             dst[j] = bad ? __longlong_as_double(0x7ff8000000000000ll) : scalbn(v, sh);
         }
     }
     if (lane == 0 && p.info) p.info[s - p.row_base] = info;
     __syncwarp();
+}
+
+template <typename T, int NMAX, int NRHS, int P, int Q, bool MIXED, int PB, bool PF>
+__device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, char* smem,
+                                             int lane) {
+    using C = BlkCfg<T, NMAX, NRHS, P, Q, MIXED, PB>;
+    constexpr int G = C::G, NP = C::NP, R = C::R, LDS = C::LDS;
+    double* cx = reinterpret_cast<double*>(smem + C::off_cx);
+    double* cy = reinterpret_cast<double*>(smem + C::off_cy);
+    T* S = reinterpret_cast<T*>(smem + C::off_s);
+    T* X = reinterpret_cast<T*>(smem + C::off_x);
+    T* pinv = reinterpret_cast<T*>(smem + C::off_pinv);
+    int* piv = reinterpret_cast<int*>(smem + C::off_piv);
+    int* act = reinterpret_cast<int*>(smem + C::off_act);
+    unsigned char* alive = reinterpret_cast<unsigned char*>(smem + C::off_alive);
+    int* nja = reinterpret_cast<int*>(smem + C::off_nja);
+    double* nxy = reinterpret_cast<double*>(smem + C::off_nxy);
+    int* nia = reinterpret_cast<int*>(smem + C::off_nia);
+
+    // With PF, stencil s was prefetched (by the previous call of this warp, or
+    // by prefetch_first): its neighbour coordinates wait in cx/cy (raw), its
+    // centre in nxy, its CSR bounds in nia. Without PF everything comes from
+    // global memory.
+    int off, ks;
+    double x0, y0;
+    if constexpr (PF) {
+        cp_async_wait_all();
+        __syncwarp();
+        x0 = nxy[0];
+        y0 = nxy[1];
+        off = p.ia ? nia[0] : (s - p.row_base) * p.k;
+        ks = p.ia ? nia[1] - off : p.k;
+        __syncwarp();  // read before the slots are refilled below
+    } else {
+        x0 = p.x[s];
+        y0 = p.y[s];
+        off = p.ia ? p.ia[s] : (s - p.row_base) * p.k;
+        ks = p.ia ? p.ia[s + 1] - off : p.k;
+    }
+    const int n = NP + ks;
+    if (PF && sn >= 0 && lane == 0) {  // prefetch stage 1: next centre and CSR bounds
+        cp_async8(nxy, p.x + sn);
+        cp_async8(nxy + 1, p.y + sn);
+        if (p.ia) {
+            cp_async4(nia, p.ia + sn);
+            cp_async4(nia + 1, p.ia + sn + 1);
+        }
+    }
+    const int e = gather_scale<C::KMAX, PF>(p, off, ks, x0, y0, cx, cy, lane);
+    fill_system<T, LDS, NRHS, P, Q>(p, S, cx, cy, ks, e, alive, NMAX, lane);
+
+    // prefetch stage 2: the next stencil's ja row (its bounds have landed)
+    if constexpr (PF) {
+        int offn = 0, ksn = 0;
+        if (sn >= 0) {
+            if (p.ia) {
+                cp_async_wait_all();
+                __syncwarp();
+                offn = nia[0];
+                ksn = nia[1] - offn;
+            } else {
+                offn = (sn - p.row_base) * p.k;
+                ksn = p.k;
+            }
+            for (int j = lane; j < ksn; j += G) cp_async4(nja + j, p.ja + offn + j);
+        }
+        __syncwarp();
+        if (lane == 0) nia[2] = ksn;
+    }
+    __syncwarp();
+
+    const int info = eliminate_blocked<T, R, LDS, NRHS, PB>(S, pinv, piv, act, alive, n, lane);
+
+    // prefetch stage 3: the next stencil's neighbour coordinates into cx/cy
+    if (const int ksn = PF ? nia[2] : 0; ksn > 0) {
+        cp_async_wait_all();
+        for (int j = lane; j < ksn; j += G) {
+            const int nb = nja[j];
+            cp_async8(cx + j, p.x + nb);
+            cp_async8(cy + j, p.y + nb);
+        }
+    }
+    back_substitute_blk<T, R, LDS, NRHS>(S, pinv, piv, X, n, lane);
+    scatter_blk<T, NRHS>(p, X, NP, ks, off, e, info, s, lane);
 }
 
 template <typename T, int NMAX, int NRHS, int P, int Q, bool MIXED, int BLOCK, int MINB, int PB,
@@ -521,6 +573,101 @@ __global__ void __launch_bounds__(BLOCK, MINB) blk_kernel(AsmParams p) {
         assemble_blk<T, NMAX, NRHS, P, Q, MIXED, PB, PF>(p, item(it), PF ? item(itn) : -1, smem, lane);
         it = *next_it;
         __syncwarp();
+    }
+}
+
+// ---- one persistent launch for an uneven batch ------------------------------
+//
+// Ragged stencils in CSR form, each with its own size k_s = ia[s+1] - ia[s],
+// degree P_s (degree[s], or P0 for all) and PHS exponent Q_s = phs, or
+// 2 P_s - 1 when phs = 0: the reference's one-grid-over-all-stencils launch
+// (src/rbf_operators.h:197-200,340) for stencils of any mix of shapes. Warps
+// claim stencils from one device work counter. A system of up to NS unknowns
+// is solved in the warp's shared-memory slot; a larger one (up to NG) in the
+// warp's region of a global scratch buffer, which stays in L2. Supported:
+// P_s in 1..4 and Q_s in {3, 5, 7, 9}; a stencil outside that (or above NG
+// unknowns, or with no neighbour) sets *err and is skipped.
+
+// Runtime-Q dispatch of the fill (the elimination does not depend on P or Q).
+template <typename T, int LDS, int NRHS, int P>
+__device__ __forceinline__ void fill_system_q(const AsmParams& p, int Q, T* S, const double* cx,
+                                              const double* cy, int ks, int e,
+                                              unsigned char* alive, int nmax, int lane) {
+    switch (Q) {
+        case 3: fill_system<T, LDS, NRHS, P, 3>(p, S, cx, cy, ks, e, alive, nmax, lane); break;
+        case 5: fill_system<T, LDS, NRHS, P, 5>(p, S, cx, cy, ks, e, alive, nmax, lane); break;
+        case 7: fill_system<T, LDS, NRHS, P, 7>(p, S, cx, cy, ks, e, alive, nmax, lane); break;
+        default: fill_system<T, LDS, NRHS, P, 9>(p, S, cx, cy, ks, e, alive, nmax, lane); break;
+    }
+}
+
+// One stencil in the working set `base` (layout L): gather, fill, eliminate,
+// back-substitute, scatter.
+template <typename T, class L, int NRHS, int PB>
+__device__ __forceinline__ void assemble_any(const AsmParams& p, int s, int off, int ks, int P,
+                                             int Q, char* base, int lane) {
+    constexpr int LDS = L::LDS;
+    double* cx = reinterpret_cast<double*>(base + L::off_cx);
+    double* cy = reinterpret_cast<double*>(base + L::off_cy);
+    T* S = reinterpret_cast<T*>(base + L::off_s);
+    T* X = reinterpret_cast<T*>(base + L::off_x);
+    T* pinv = reinterpret_cast<T*>(base + L::off_pinv);
+    int* piv = reinterpret_cast<int*>(base + L::off_piv);
+    int* act = reinterpret_cast<int*>(base + L::off_act);
+    unsigned char* alive = reinterpret_cast<unsigned char*>(base + L::off_alive);
+    const int np = npoly(P), n = np + ks;
+    const int e = gather_scale<L::KMAX, false>(p, off, ks, p.x[s], p.y[s], cx, cy, lane);
+    switch (P) {
+        case 1: fill_system_q<T, LDS, NRHS, 1>(p, Q, S, cx, cy, ks, e, alive, n, lane); break;
+        case 2: fill_system_q<T, LDS, NRHS, 2>(p, Q, S, cx, cy, ks, e, alive, n, lane); break;
+        case 3: fill_system_q<T, LDS, NRHS, 3>(p, Q, S, cx, cy, ks, e, alive, n, lane); break;
+        default: fill_system_q<T, LDS, NRHS, 4>(p, Q, S, cx, cy, ks, e, alive, n, lane); break;
+    }
+    __syncwarp();
+    const int info = eliminate_blocked<T, L::R, LDS, NRHS, PB>(S, pinv, piv, act, alive, n, lane);
+    back_substitute_blk<T, L::R, LDS, NRHS>(S, pinv, piv, X, n, lane);
+    scatter_blk<T, NRHS>(p, X, np, ks, off, e, info, s, lane);
+}
+
+template <typename T, int NS, int NG, int NRHS, int PB>
+struct CsrCfg {
+    using SmemL = BlkLayout<T, NS, NRHS, NS, PB>;    // shared-memory slot
+    using GlobL = BlkLayout<T, NG, NRHS, NG, PB>;    // global scratch region
+    static constexpr size_t gbytes = (static_cast<size_t>(GlobL::bytes) + 255) & ~size_t(255);
+};
+
+template <typename T, int NS, int NG, int NRHS, int BLOCK, int PB>
+__global__ void __launch_bounds__(BLOCK, 1)
+    blk_csr_kernel(AsmParams p, const int8_t* degree, int P0, int phs, char* gscratch, int* err) {
+    using C = CsrCfg<T, NS, NG, NRHS, PB>;
+    constexpr int GPB = BLOCK / 32;
+    extern __shared__ __align__(16) char smem_raw[];
+    const int gib = threadIdx.x / 32;
+    const int lane = threadIdx.x % 32;
+    char* slot = smem_raw + gib * C::SmemL::bytes;
+    char* gslot = gscratch + (static_cast<size_t>(blockIdx.x) * GPB + gib) * C::gbytes;
+    const int nitems = p.nitems_dev ? *p.nitems_dev : p.nitems;
+    const int* list = (p.list && p.list_off_dev) ? p.list + *p.list_off_dev : p.list;
+    for (;;) {
+        int it = 0;
+        if (lane == 0) it = atomicAdd(p.work, 1);
+        it = __shfl_sync(0xffffffffu, it, 0);
+        if (it >= nitems) break;
+        const int s = list ? list[it] : p.item_base + it;
+        const int off = p.ia[s], ks = p.ia[s + 1] - off;
+        const int P = degree ? degree[s] : P0;
+        const int Q = phs ? phs : 2 * P - 1;
+        const int n = ks + npoly(P);
+        const bool ok = P >= 1 && P <= 4 && (Q == 3 || Q == 5 || Q == 7 || Q == 9) && ks >= 1 &&
+                        n <= NG;
+        if (!ok) {
+            if (lane == 0) atomicExch(err, 1);
+            continue;
+        }
+        if (n <= NS)
+            assemble_any<T, typename C::SmemL, NRHS, PB>(p, s, off, ks, P, Q, slot, lane);
+        else
+            assemble_any<T, typename C::GlobL, NRHS, PB>(p, s, off, ks, P, Q, gslot, lane);
     }
 }
 

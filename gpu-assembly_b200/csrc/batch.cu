@@ -1,13 +1,19 @@
 // batch.cu -- uneven stencils: rbfb_assemble_csr.
 //
-// Stencils of different size and degree (interior vs boundary, k from 21 to
-// 64, degree 2 to 4) are bucketed on the device by the compiled kernel shape
-// that fits them (smallest padded system size >= k + npoly(P)), counting-
-// sorted into one stencil list, and each bucket's persistent kernel walks its
-// slice of the list. Bucket sizes and offsets stay on the device (kernels
-// read them through pointers), so the whole call is a fixed sequence of
-// launches with no host round trip; the sequence is captured once into a CUDA
-// graph and replayed for the same batch.
+// FP64 batches (up to 3 right-hand sides) run as ONE persistent launch of the
+// uneven kernel (asm_blocked.cuh, blk_csr_kernel): warps claim stencils of
+// any size and degree from a device counter; systems of up to 48 unknowns
+// are solved in shared memory, larger ones (up to 96) in an L2-resident
+// global scratch region per warp.
+//
+// Other batches (the FP32-refinement form, more right-hand sides) are
+// bucketed on the device by the compiled kernel shape that fits them
+// (smallest padded system size >= k + npoly(P)), counting-sorted into one
+// stencil list, and each bucket's persistent kernel walks its slice of the
+// list. Bucket sizes and offsets stay on the device (kernels read them
+// through pointers), so the whole call is a fixed sequence of launches with
+// no host round trip; the sequence is captured once into a CUDA graph and
+// replayed for the same batch.
 //
 // The reference's only CSR-driven assembly is the Fortran fill_kernel over
 // ia/ja (src/rbf_cuda.f90:36-99); its C++ kernel takes one fixed stencil size
@@ -19,10 +25,17 @@
 #include <cstring>
 #include <vector>
 
+#include "asm_blocked.cuh"
 #include "runtime.h"
 
 namespace rbfb {
 namespace {
+
+// The single-launch FP64 kernel for uneven batches: systems of up to 48
+// unknowns in shared memory (three warps per CTA), up to 96 in global scratch.
+constexpr int kOneNS = 48, kOneNG = 96, kOneBlock = 96, kOnePB = 8;
+using OneCfg = CsrCfg<double, kOneNS, kOneNG, 3, kOnePB>;
+constexpr int kOneSmem = OneCfg::SmemL::bytes * (kOneBlock / 32);
 
 constexpr int kMaxVariants = 64;
 constexpr int kTabN = 161;  // system sizes 0..160
@@ -38,6 +51,10 @@ struct BatchState {
     size_t cap = 0;
     int* bucket_of = nullptr;
     int* list = nullptr;
+    // the single-launch kernel: persistent grid and its global scratch
+    int one_grid = 0;
+    char* gscratch = nullptr;
+    size_t gscratch_bytes = 0;
     // cached graph of the last batch
     cudaGraphExec_t graph = nullptr;
     std::vector<unsigned char> graph_key;
@@ -132,7 +149,31 @@ int build_table(rbfb_ctx* ctx, BatchState* b, bool mixed, int phs, int Pmin, int
     return RBFB_OK;
 }
 
+// Grid and global scratch of the single-launch kernel (set up outside any
+// stream capture).
+int ensure_one(rbfb_ctx* ctx, BatchState* b) {
+    const void* k = reinterpret_cast<const void*>(
+        &blk_csr_kernel<double, kOneNS, kOneNG, 3, kOneBlock, kOnePB>);
+    if (b->one_grid == 0) {
+        RBFB_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kOneSmem));
+        int nb = 0;
+        RBFB_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k, kOneBlock, kOneSmem));
+        if (nb < 1) return fail(ctx, RBFB_EUNSUPPORTED, "uneven kernel does not fit an SM");
+        b->one_grid = nb * ctx->sms;
+    }
+    const size_t need = static_cast<size_t>(b->one_grid) * (kOneBlock / 32) * OneCfg::gbytes;
+    if (b->gscratch_bytes < need) {
+        cudaFree(b->gscratch);
+        b->gscratch = nullptr;
+        b->gscratch_bytes = 0;
+        RBFB_CUDA(ctx, cudaMalloc(&b->gscratch, need));
+        b->gscratch_bytes = need;
+    }
+    return RBFB_OK;
+}
+
 void release(BatchState* b) {
+    cudaFree(b->gscratch);
     cudaFree(b->table); cudaFree(b->counts); cudaFree(b->ctrs); cudaFree(b->err);
     cudaFree(b->bucket_of); cudaFree(b->list);
     if (b->graph) cudaGraphExecDestroy(b->graph);
@@ -166,17 +207,27 @@ int rbfb_assemble_csr(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const
     rc = ensure(ctx, b, static_cast<size_t>(std::max(nstencils, 1)));
     if (rc) return rc;
     const bool mixed = desc->precision == RBFB_FP32_IR;
-    std::vector<int> used;
-    rc = build_table(ctx, b, mixed, desc->phs, degree ? 0 : desc->degree,
-                     degree ? 4 : desc->degree, used);
-    if (rc) return rc;
-    if (used.empty()) return fail(ctx, RBFB_EUNSUPPORTED, "no compiled kernel for these degrees");
 
     // the parameters every bucket shares
     AsmParams p;
     std::memset(&p, 0, sizeof(p));
     const int nrhs = rhs_columns(desc, p);
     if (nrhs < 0) return fail(ctx, nrhs, "bad operator mask / interpolation points");
+    // FP64 with up to 3 right-hand sides: the whole batch in ONE persistent
+    // launch of the uneven kernel; otherwise bucketed launches
+    const bool one = !mixed && nrhs <= 3 &&
+                     (desc->phs == 0 || desc->phs == 3 || desc->phs == 5 || desc->phs == 7 ||
+                      desc->phs == 9);
+    std::vector<int> used;
+    if (one) {
+        rc = ensure_one(ctx, b);
+        if (rc) return rc;
+    } else {
+        rc = build_table(ctx, b, mixed, desc->phs, degree ? 0 : desc->degree,
+                         degree ? 4 : desc->degree, used);
+        if (rc) return rc;
+        if (used.empty()) return fail(ctx, RBFB_EUNSUPPORTED, "no compiled kernel for these degrees");
+    }
     for (int q = 0; q < nrhs; ++q) {
         if (!values_h[q]) return fail(ctx, RBFB_EINVAL, "null values pointer");
         p.values[q] = values_h[q];
@@ -212,8 +263,25 @@ int rbfb_assemble_csr(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const
         }
         if (nrhs > variants()[v].nrhs) return fail(ctx, RBFB_EUNSUPPORTED, "too many right-hand sides");
     }
+    // the whole batch in one launch: warps claim stencils from a counter
+    auto enqueue_one = [&](cudaStream_t s) -> int {
+        RBFB_CUDA(ctx, cudaMemsetAsync(b->ctrs, 0, kMaxVariants * sizeof(DevCounters), s));
+        RBFB_CUDA(ctx, cudaMemsetAsync(b->err, 0, sizeof(int), s));
+        if (nstencils == 0) return RBFB_OK;
+        AsmParams q = p;
+        q.list = nullptr;
+        q.item_base = 0;
+        q.nitems = nstencils;
+        q.work = &b->ctrs[0].work[0];
+        blk_csr_kernel<double, kOneNS, kOneNG, 3, kOneBlock, kOnePB>
+            <<<b->one_grid, kOneBlock, kOneSmem, s>>>(q, degree, desc->degree, desc->phs,
+                                                       b->gscratch, b->err);
+        ctx->launches += 1;
+        RBFB_CUDA(ctx, cudaGetLastError());
+        return RBFB_OK;
+    };
     // the whole batch: a fixed sequence of launches, sizes read on the device
-    auto enqueue = [&](cudaStream_t s) -> int {
+    auto enqueue_buckets = [&](cudaStream_t s) -> int {
         RBFB_CUDA(ctx, cudaMemsetAsync(b->counts, 0, 3 * kMaxVariants * sizeof(int), s));
         RBFB_CUDA(ctx, cudaMemsetAsync(b->ctrs, 0, kMaxVariants * sizeof(DevCounters), s));
         RBFB_CUDA(ctx, cudaMemsetAsync(b->err, 0, sizeof(int), s));
@@ -247,6 +315,7 @@ int rbfb_assemble_csr(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const
         }
         return RBFB_OK;
     };
+    auto enqueue = [&](cudaStream_t s) -> int { return one ? enqueue_one(s) : enqueue_buckets(s); };
     // Captured into a CUDA graph on a non-default stream, replayed while the
     // arguments (and the context's buffers) stay the same.
     if (st != nullptr) {
@@ -256,12 +325,13 @@ int rbfb_assemble_csr(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const
             key.insert(key.end(), c, c + len);
         };
         const void* ptrs[] = {x, y, ia, ja, degree, info, b->list, b->bucket_of, b->counts,
-                              b->ctrs, ctx->fb_list, b->table};
+                              b->ctrs, ctx->fb_list, b->table, b->gscratch};
         put(ptrs, sizeof(ptrs));
         put(p.values, sizeof(p.values));
         put(&nstencils, sizeof(nstencils));
         put(desc, offsetof(rbfb_desc, nc));
         put(&desc->nc, sizeof(desc->nc));
+        put(&one, sizeof(one));
         if (!b->graph || key != b->graph_key) {
             if (b->graph) cudaGraphExecDestroy(b->graph);
             b->graph = nullptr;
@@ -312,7 +382,7 @@ int rbfb_assemble_csr(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const
         stats->sweeps += static_cast<long long>(c.sweeps_sum);
         stats->max_sweeps_used = std::max(stats->max_sweeps_used, c.sweeps_max);
     }
-    stats->buckets = static_cast<int>(used.size());
+    stats->buckets = one ? 1 : static_cast<int>(used.size());
     stats->ms = ms;
     if (herr) return fail(ctx, RBFB_EUNSUPPORTED, "a stencil has no compiled kernel (size or degree)");
     return RBFB_OK;

@@ -61,6 +61,10 @@ struct Req {
     long long singular = 0, fallback = 0;
     bool counted = false;
     double t_submit = 0, t_start = 0, t_end = 0;
+    // device clock: events around the request's work on its stream, read
+    // against the server's origin event once the request is done
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double dev_start = -1.0, dev_end = -1.0;
     Slot* slot = nullptr;
     cudaStream_t stream = nullptr;
 };
@@ -88,6 +92,7 @@ struct rbfb_server {
     std::deque<long long> queue;
     Clock::time_point t0 = Clock::now();
     cudaStream_t io = nullptr;  // fetch copies
+    cudaEvent_t origin = nullptr;  // device-clock origin of the requests' timings
     // Pinned staging buffers for submitted node sets, reused: page-locking
     // and unlocking host memory per request costs milliseconds (and
     // unlocking may wait for the device). Blocks are never returned to the
@@ -182,6 +187,9 @@ int launch(rbfb_server* s, Slot& sl, Req* r) {
     e = cudaMemcpyAsync(r->x, r->xh, n * 8, cudaMemcpyHostToDevice, st);
     e = e ? e : cudaMemcpyAsync(r->y, r->yh, n * 8, cudaMemcpyHostToDevice, st);
     e = e ? e : cudaMemsetAsync(r->ctr, 0, sizeof(rbfb::DevCounters), st);
+    e = e ? e : cudaEventCreate(&r->ev0);
+    e = e ? e : cudaEventCreate(&r->ev1);
+    e = e ? e : cudaEventRecord(r->ev0, st);  // the request's kernels start after this point
     if (e) return RBFB_ECUDA;
     rbfb_ctx* ctx = sl.ctx;
     const double per[2] = {r->desc.period[0], r->desc.period[1]};
@@ -197,7 +205,8 @@ int launch(rbfb_server* s, Slot& sl, Req* r) {
         if (rc >= 0) rc = rbfb::count_singular(ctx, r->info, r->n, &r->ctr->singular, st);
     }
     if (rc < 0) return rc;
-    e = cudaLaunchHostFunc(st, on_done, new CallbackArg{s, r});
+    e = cudaEventRecord(r->ev1, st);
+    e = e ? e : cudaLaunchHostFunc(st, on_done, new CallbackArg{s, r});
     return e ? RBFB_ECUDA : RBFB_OK;
 }
 
@@ -258,6 +267,9 @@ void free_request(rbfb_server* s, Req* r) {
     };
     fr(r->x); fr(r->y); fr(r->ja); fr(r->info); fr(r->fb); fr(r->ctr);
     for (auto& v : r->vals) fr(v);
+    if (r->ev0) cudaEventDestroy(r->ev0);
+    if (r->ev1) cudaEventDestroy(r->ev1);
+    r->ev0 = r->ev1 = nullptr;
     // staging of a request that never completed (failed or never launched)
     pin_release(s, r->xh, r->xh_cap);
     pin_release(s, r->yh, r->yh_cap);
@@ -288,6 +300,15 @@ int rbfb_server_create(rbfb_server** out, int device, size_t budget, int max_slo
         }
     }
     cudaStreamCreateWithFlags(&s->io, cudaStreamNonBlocking);
+    if (cudaEventCreate(&s->origin) != cudaSuccess || cudaEventRecord(s->origin, s->io) != cudaSuccess ||
+        cudaEventSynchronize(s->origin) != cudaSuccess) {
+        for (auto& t : s->slots) {
+            rbfb_destroy(t.ctx);
+            cudaStreamDestroy(t.stream);
+        }
+        delete s;
+        return RBFB_ECUDA;
+    }
     // Requests allocate from the device's default stream-ordered pool; let it
     // keep up to the budget cached between requests instead of handing memory
     // back to the driver at every synchronisation (an attribute of this
@@ -363,10 +384,17 @@ int rbfb_server_poll(rbfb_server* s, long long ticket, int wait_ms, rbfb_result*
     // without the lock)
     if (r->state == State::Done && !r->counted && r->ctr) {
         rbfb::DevCounters h{};
+        float a = -1.f, b = -1.f;
+        if (r->ev0 && r->ev1) {
+            if (cudaEventElapsedTime(&a, s->origin, r->ev0) != cudaSuccess) a = -1.f;
+            if (cudaEventElapsedTime(&b, s->origin, r->ev1) != cudaSuccess) b = -1.f;
+        }
         if (cudaMemcpy(&h, r->ctr, sizeof(h), cudaMemcpyDeviceToHost) == cudaSuccess) {
             std::lock_guard<std::mutex> l(s->mu);
             r->singular = static_cast<long long>(h.singular);
             r->fallback = h.fb_count;
+            r->dev_start = a;
+            r->dev_end = b;
             r->counted = true;
         }
     }
@@ -384,6 +412,8 @@ int rbfb_server_poll(rbfb_server* s, long long ticket, int wait_ms, rbfb_result*
         res->submit_ms = r->t_submit;
         res->start_ms = r->t_start;
         res->end_ms = r->t_end;
+        res->dev_start_ms = r->dev_start;
+        res->dev_end_ms = r->dev_end;
     }
     return r->state == State::Failed ? r->status : RBFB_OK;
 }
@@ -451,6 +481,7 @@ int rbfb_server_destroy(rbfb_server* s) {
         rbfb_destroy(sl.ctx);
     }
     if (s->io) cudaStreamDestroy(s->io);
+    if (s->origin) cudaEventDestroy(s->origin);
     for (void* p : s->pin_all) cudaFreeHost(p);
     delete s;
     return RBFB_OK;

@@ -73,7 +73,8 @@ class Result(C.Structure):
     _fields_ = [("status", C.c_int), ("n", C.c_int), ("k", C.c_int), ("nrhs", C.c_int),
                 ("singular", C.c_longlong), ("fallback", C.c_longlong),
                 ("ja", C.c_void_p), ("values", C.c_void_p * MAX_RHS),
-                ("submit_ms", C.c_double), ("start_ms", C.c_double), ("end_ms", C.c_double)]
+                ("submit_ms", C.c_double), ("start_ms", C.c_double), ("end_ms", C.c_double),
+                ("dev_start_ms", C.c_double), ("dev_end_ms", C.c_double)]
 
 
 _lib = None

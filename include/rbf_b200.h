@@ -410,6 +410,9 @@ typedef struct rbfb_result {
     const int* ja;           /* DEVICE, n*k, resident until rbfb_server_release    */
     const double* values[RBFB_MAX_RHS]; /* DEVICE, n*k each                         */
     double submit_ms, start_ms, end_ms; /* host clock, relative to server creation  */
+    double dev_start_ms, dev_end_ms;    /* device clock, same origin: when the request's
+                                           kernels could start and when they finished
+                                           (-1 until the request is done)             */
 } rbfb_result;
 
 int rbfb_server_create(rbfb_server** srv, int device, size_t hbm_budget_bytes, int max_slots);

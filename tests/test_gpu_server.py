@@ -69,3 +69,34 @@ def test_budget_and_bounded_waits(torch_cuda):
         assert srv.release(t) == 0
     finally:
         srv.close()
+
+
+def test_requests_overlap_on_the_device(torch_cuda):
+    """Continuous batching: requests submitted together run in different
+    slots at the same time, so on the device clock (events around each
+    request's kernels) some request's work starts before another's ends.
+    Each result still equals the one computed alone (bit for bit)."""
+    reqs = []
+    for i in range(4):
+        req = dict(n=250 * 250, geometry="square", k=35, P=3, Q=5, seed=300 + i)
+        x, y = NS.request_nodes(req)
+        reqs.append((x, y, 35, 3))
+    srv = R.Server(0, hbm_budget=4 << 30, max_slots=4)
+    try:
+        tickets = [srv.submit(x, y, k, R.make_desc(P)) for x, y, k, P in reqs]
+        wins = []
+        for t, (x, y, k, P) in zip(tickets, reqs):
+            st, res = srv.poll(t, wait_ms=60000)
+            assert st == 0 and res.status == 0
+            assert 0.0 <= res.dev_start_ms <= res.dev_end_ms
+            wins.append((res.dev_start_ms, res.dev_end_ms))
+            vals, _ = srv.fetch(t, x.size, k, 3)
+            _, vals1 = run_alone(x, y, k, P, R.FP64)
+            for a, b in zip(vals, vals1):
+                np.testing.assert_array_equal(a, b)
+            assert srv.release(t) == 0
+        overlapping = [(i, j) for i in range(4) for j in range(i + 1, 4)
+                       if wins[i][0] < wins[j][1] and wins[j][0] < wins[i][1]]
+        assert overlapping, f"no two requests overlapped on the device: {wins}"
+    finally:
+        srv.close()
