@@ -411,30 +411,34 @@ __device__ __forceinline__ void back_substitute_blk(const T* S, const T* pinv, c
 #pragma unroll
         for (int q = 0; q < NRHS; ++q) y[sl][q] = t < n ? S[prow_t[sl] * LDS + n + q] : T(0);
     }
+    // Steps in segments of 32 from the last: in segment OS the owner of step c
+    // holds it in slot OS (static), the slots below OS hold steps all before
+    // c (updated unconditionally), the slots above OS steps all after it.
+    auto segment = [&](auto os_c) {
+        constexpr int OS = decltype(os_c)::value;
 #pragma unroll 1
-    for (int c = n - 1; c >= 0; --c) {
-        const int owner = c & (G - 1), osl = c / G;
-        const T dv = pinv[c];
-        T xq[NRHS];
+        for (int c = min(n, G * (OS + 1)) - 1; c >= G * OS; --c) {
+            const T dv = pinv[c];
+            T xq[NRHS];
 #pragma unroll
-        for (int q = 0; q < NRHS; ++q) {
-            T v = y[0][q];
+            for (int q = 0; q < NRHS; ++q) xq[q] = __shfl_sync(FULL, y[OS][q] * dv, c - G * OS);
+            if (lane == 0) {
 #pragma unroll
-            for (int sl = 1; sl < R; ++sl) v = (osl == sl) ? y[sl][q] : v;
-            xq[q] = __shfl_sync(FULL, v * dv, owner);
+                for (int q = 0; q < NRHS; ++q) X[c * NRHS + q] = xq[q];
+            }
+#pragma unroll
+            for (int sl = 0; sl <= OS; ++sl) {
+                T u = S[prow_t[sl] * LDS + c];
+                if (sl == OS) u = (lane + G * sl < c) ? u : T(0);
+#pragma unroll
+                for (int q = 0; q < NRHS; ++q) y[sl][q] = fma(-u, xq[q], y[sl][q]);
+            }
         }
-        if (lane == 0) {
-#pragma unroll
-            for (int q = 0; q < NRHS; ++q) X[c * NRHS + q] = xq[q];
-        }
-#pragma unroll
-        for (int sl = 0; sl < R; ++sl) {
-            const int t = lane + G * sl;
-            const T u = (t < c) ? S[prow_t[sl] * LDS + c] : T(0);
-#pragma unroll
-            for (int q = 0; q < NRHS; ++q) y[sl][q] = fma(-u, xq[q], y[sl][q]);
-        }
-    }
+    };
+    if constexpr (R > 3) segment(std::integral_constant<int, 3>{});
+    if constexpr (R > 2) segment(std::integral_constant<int, 2>{});
+    if constexpr (R > 1) segment(std::integral_constant<int, 1>{});
+    segment(std::integral_constant<int, 0>{});
     __syncwarp();
 }
 

@@ -70,7 +70,8 @@ int pick_variant(rbfb_ctx* ctx, bool mixed, int P, int Q, int n, int nrhs) {
     if (best_ntp == (1 << 30)) return -1;
     if (ctx) {
         auto it = ctx->tuned.find({mixed ? 1 : 0, P, Q, best_ntp});
-        if (it != ctx->tuned.end() && it->second.variant >= 0 && serves(vs[it->second.variant]))
+        if (it != ctx->tuned.end() && it->second.variant >= 0 && serves(vs[it->second.variant]) &&
+            vs[it->second.variant].ntp >= n)
             return it->second.variant;
     }
     for (size_t i = 0; i < vs.size(); ++i)
@@ -100,12 +101,15 @@ int grid_for(rbfb_ctx* ctx, int v, int bps_override) {
 int launch_variant(rbfb_ctx* ctx, int v, const AsmParams& p, cudaStream_t st, int blocks) {
     const auto& var = variants()[v];
     if (blocks <= 0) {
-        // a tuned CTAs-per-SM for this shape, if the autotuner chose one
-        auto it = ctx->tuned.find({var.mixed ? 1 : 0, var.P, var.Q, var.ntp});
-        if (it != ctx->tuned.end() && it->second.variant == v && it->second.blocks_per_sm > 0) {
-            const int g = grid_for(ctx, v, it->second.blocks_per_sm);
-            if (g < 0) return g;
-            blocks = g;
+        // a tuned CTAs-per-SM for this shape, if the autotuner chose one (the
+        // entry sits under the smallest system size of its class)
+        for (const auto& kv : ctx->tuned) {
+            if (kv.second.variant == v && kv.second.blocks_per_sm > 0) {
+                const int g = grid_for(ctx, v, kv.second.blocks_per_sm);
+                if (g < 0) return g;
+                blocks = g;
+                break;
+            }
         }
     }
     int grid = blocks > 0 ? blocks : grid_for(ctx, v);

@@ -37,7 +37,7 @@ int rbfb_select_variant(rbfb_ctx* ctx, const rbfb_desc* desc, int k, int index,
     for (const auto& v : vs)
         if (v.mixed == mixed && v.P == P && v.Q == Q && v.ntp >= n) ntp = std::min(ntp, v.ntp);
     const auto& v = vs[index];
-    if (v.mixed != mixed || v.P != P || v.Q != Q || v.ntp != ntp)
+    if (v.mixed != mixed || v.P != P || v.Q != Q || v.ntp < n)
         return fail(ctx, RBFB_EINVAL, std::string("shape ") + v.name +
                                           " does not serve this precision, degree, PHS and size");
     std::lock_guard<std::mutex> lock(ctx->mu);
@@ -56,14 +56,17 @@ int rbfb_autotune(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const dou
     const int Q = desc->phs ? desc->phs : 2 * P - 1;
     const int n = k + npoly(P);
     const bool mixed = desc->precision == RBFB_FP32_IR;
-    // candidate shapes: the smallest padded size that fits, every layout
+    // candidate shapes: every layout whose system size fits, up to 16 above
+    // the smallest that does (a larger slot can still win on code shape);
+    // the choice is recorded under the smallest size, where pick_variant looks
     const auto& vs = variants();
     int ntp = 1 << 30;
     for (const auto& v : vs)
         if (v.mixed == mixed && v.P == P && v.Q == Q && v.ntp >= n) ntp = std::min(ntp, v.ntp);
     std::vector<int> cands;
     for (size_t i = 0; i < vs.size(); ++i)
-        if (vs[i].mixed == mixed && vs[i].P == P && vs[i].Q == Q && vs[i].ntp == ntp)
+        if (vs[i].mixed == mixed && vs[i].P == P && vs[i].Q == Q && vs[i].ntp >= n &&
+            vs[i].ntp <= ntp + 16)
             cands.push_back(static_cast<int>(i));
     if (cands.empty()) return fail(ctx, RBFB_EUNSUPPORTED, "no compiled kernel for this shape");
     cudaStream_t st = nullptr;
