@@ -47,3 +47,34 @@ def test_reference_arm_line():
     assert line["warmup"] >= 3  # the timing rules' minimum
     assert line["cpu_baseline"]["cores"] >= 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0
+
+
+def test_sampled_oracle_matches_the_full_oracle():
+    """bench.sampled_oracle renumbers the nodes so the sampled centres come
+    first and assembles just those stencils: it must give the weights the
+    full oracle gives for those stencils, also for ragged rows and for rows
+    of a rank's range (centres offset from the rows)."""
+    import numpy as np
+    import oracle as O
+    from rbf_b200 import nodesets as NS
+    x, y, _ = NS.jittered_grid(24, 0.3, seed=3)
+    n, k = x.size, 21
+    ja = O.knn_brute(x, y, k)
+    Wfull, _ = O.assemble(x, y, ja, k, 2)
+    rows = np.array([5, 77, 300, 511])
+    ia = np.arange(n + 1, dtype=np.int64) * k
+    W, ia_s = bench.sampled_oracle(O, x, y, ia, ja, rows, P_=2, Q_=3)
+    idx = (rows[:, None] * k + np.arange(k)[None, :]).ravel()
+    np.testing.assert_array_equal(W, Wfull[:, idx])
+    assert bench.ragged_rel_err(W, Wfull[:, idx], ia_s) == 0.0
+    # a rank holding rows 100.. of the node set: local rows, global centres
+    first = 100
+    W2, _ = bench.sampled_oracle(O, x, y, ia[:n - first + 1], ja[first * k:], rows[:2], P_=2,
+                                 Q_=3, centres=rows[:2] + first)
+    idx2 = ((rows[:2] + first)[:, None] * k + np.arange(k)[None, :]).ravel()
+    np.testing.assert_array_equal(W2, Wfull[:, idx2])
+
+
+def test_lbm_byte_model():
+    # ja row, 8 weight rows, 9 populations in and out, 3 moments out
+    assert bench.lbm_bytes_per_node(21) == 4 * 21 + 64 * 21 + 72 + 72 + 24 == 1596
