@@ -87,8 +87,19 @@ struct BlkLayout {
 
 template <typename T, int NMAX, int NRHS, int P, int Q, bool MIXED, int PB>
 struct BlkCfg : BlkLayout<T, NMAX, NRHS, NMAX - npoly(P), PB> {
-    static_assert(!MIXED, "the blocked kernel is FP64");
+    using L = BlkLayout<T, NMAX, NRHS, NMAX - npoly(P), PB>;
+    static_assert(MIXED ? sizeof(T) == 4 : sizeof(T) == 8,
+                  "FP64 factors for the plain form, FP32 factors for the refined one");
     static constexpr int NP = npoly(P);
+    // FP64 copies the refinement reads (MIXED only): phi (packed strict upper
+    // triangle of the node block), the monomials of the nodes, the solution
+    // and the right-hand sides
+    static constexpr int NPAIR = L::KMAX * (L::KMAX - 1) / 2;
+    static constexpr int off_phi = L::bytes;
+    static constexpr int off_pm = off_phi + (MIXED ? L::al16(8 * NPAIR) : 0);
+    static constexpr int off_x64 = off_pm + (MIXED ? L::al16(8 * L::KMAX * NP) : 0);
+    static constexpr int off_b64 = off_x64 + (MIXED ? L::al16(8 * NMAX * NRHS) : 0);
+    static constexpr int bytes = off_b64 + (MIXED ? L::al16(8 * NMAX * NRHS) : 0);
 };
 
 // 16-byte vector moves between shared memory and register arrays.
@@ -172,10 +183,15 @@ __device__ __forceinline__ int gather_scale(const AsmParams& p, int off, int ks,
 // once, a flat walk over the lanes), monomial rows and columns, zero
 // polynomial block, right-hand sides as columns n .. n+NRHS-1 (fill_matrix /
 // fill_rhs, src/rbf_operators.h:116-185); alive[r] = r < n for r < nmax.
+// With phi != nullptr (the refined form) the FP64 values are also kept: phi
+// (pair (i, j), i < j, at its number in row-major order of the strict upper
+// triangle), pm[i*NP + m] (monomials of node i) and b64[r*NRHS + q].
 template <typename T, int LDS, int NRHS, int P, int Q>
 __device__ __forceinline__ void fill_system(const AsmParams& p, T* S, const double* cx,
                                             const double* cy, int ks, int e,
-                                            unsigned char* alive, int nmax, int lane) {
+                                            unsigned char* alive, int nmax, int lane,
+                                            double* phi = nullptr, double* pm = nullptr,
+                                            double* b64 = nullptr) {
     constexpr int G = 32, NP = npoly(P);
     const int n = NP + ks;
     {
@@ -186,9 +202,11 @@ __device__ __forceinline__ void fill_system(const AsmParams& p, T* S, const doub
             ++i;
         }
         for (int t = lane; t < npair; t += G) {
-            const T v = static_cast<T>(phs64<Q>(dist2(dsub(cx[j], cx[i]), dsub(cy[j], cy[i]))));
+            const double v64 = phs64<Q>(dist2(dsub(cx[j], cx[i]), dsub(cy[j], cy[i])));
+            const T v = static_cast<T>(v64);
             S[(NP + i) * LDS + NP + j] = v;
             S[(NP + j) * LDS + NP + i] = v;
+            if (phi) phi[t] = v64;
             j += G;
             while (i < ks - 1 && j >= ks) {
                 j += i + 2 - ks;
@@ -206,18 +224,25 @@ __device__ __forceinline__ void fill_system(const AsmParams& p, T* S, const doub
         for (int m = 0; m < NP; ++m) {
             Sr[m] = static_cast<T>(mon[m]);
             S[m * LDS + r] = static_cast<T>(mon[m]);
+            if (pm) pm[i * NP + m] = mon[m];
         }
         Sr[r] = T(0);
         double rv[NRHS];
         rhs_node<P, Q, NRHS>(p, xi, yi, e, rv);
 #pragma unroll
-        for (int q = 0; q < NRHS; ++q) Sr[n + q] = static_cast<T>(rv[q]);
+        for (int q = 0; q < NRHS; ++q) {
+            Sr[n + q] = static_cast<T>(rv[q]);
+            if (b64) b64[r * NRHS + q] = rv[q];
+        }
     }
     for (int f = lane; f < NP * NP; f += G) S[(f / NP) * LDS + f % NP] = T(0);
     for (int r = lane; r < NP; r += G) {
 #pragma unroll
-        for (int q = 0; q < NRHS; ++q)
-            S[r * LDS + n + q] = static_cast<T>(q < p.nrhs ? rhs_poly<P>(p, q, r, e) : 0.0);
+        for (int q = 0; q < NRHS; ++q) {
+            const double v = q < p.nrhs ? rhs_poly<P>(p, q, r, e) : 0.0;
+            S[r * LDS + n + q] = static_cast<T>(v);
+            if (b64) b64[r * NRHS + q] = v;
+        }
     }
     for (int r = lane; r < nmax; r += G) alive[r] = r < n ? 1 : 0;
 }
@@ -442,6 +467,109 @@ __device__ __forceinline__ void back_substitute_blk(const T* S, const T* pinv, c
     __syncwarp();
 }
 
+// Forward substitution with the unit lower factor kept in S (the refined
+// form): the right-hand sides in S's columns n .. n+NRHS-1, in row order, are
+// replaced by L^-1 P b in the layout the elimination leaves them (row piv[t]
+// holds component t). Lane l holds the components of steps l, l + 32, ...;
+// for c = 0 .. n-1 the owner of step c broadcasts it by shuffle and the rows
+// pivoted after c update with their multiplier l(row, c) = S(row, c).
+template <typename T, int R, int LDS, int NRHS>
+__device__ __forceinline__ void forward_substitute_blk(T* S, const int* piv, int n, int lane) {
+    constexpr int G = 32;
+    constexpr unsigned FULL = 0xffffffffu;
+    T y[R][NRHS];
+    int prow_t[R];
+#pragma unroll
+    for (int sl = 0; sl < R; ++sl) {
+        const int t = lane + G * sl;
+        prow_t[sl] = t < n ? piv[t] : 0;
+#pragma unroll
+        for (int q = 0; q < NRHS; ++q) y[sl][q] = t < n ? S[prow_t[sl] * LDS + n + q] : T(0);
+    }
+    // segments of 32 steps from the first: in segment OS the owner of step c
+    // holds it in slot OS, the slots above OS hold steps all after c
+    auto segment = [&](auto os_c) {
+        constexpr int OS = decltype(os_c)::value;
+#pragma unroll 1
+        for (int c = G * OS; c < min(n, G * (OS + 1)); ++c) {
+            T z[NRHS];
+#pragma unroll
+            for (int q = 0; q < NRHS; ++q) z[q] = __shfl_sync(FULL, y[OS][q], c - G * OS);
+#pragma unroll
+            for (int sl = OS; sl < R; ++sl) {
+                T l = S[prow_t[sl] * LDS + c];
+                if (sl == OS) l = (lane + G * sl > c) ? l : T(0);
+#pragma unroll
+                for (int q = 0; q < NRHS; ++q) y[sl][q] = fma(-l, z[q], y[sl][q]);
+            }
+        }
+    };
+    segment(std::integral_constant<int, 0>{});
+    if constexpr (R > 1) segment(std::integral_constant<int, 1>{});
+    if constexpr (R > 2) segment(std::integral_constant<int, 2>{});
+    if constexpr (R > 3) segment(std::integral_constant<int, 3>{});
+#pragma unroll
+    for (int sl = 0; sl < R; ++sl) {
+        if (lane + G * sl < n) {
+#pragma unroll
+            for (int q = 0; q < NRHS; ++q) S[prow_t[sl] * LDS + n + q] = y[sl][q];
+        }
+    }
+    __syncwarp();
+}
+
+// Packed index of the pair (i, j), i < j, of a k-node stencil.
+__device__ __forceinline__ int tri_idx(int i, int j, int k) {
+    return i * (2 * k - i - 1) / 2 + (j - i - 1);
+}
+
+// FP64 residual b - M x of the refined form, from the FP64 copies, rounded to
+// T into S's right-hand-side columns (row order).
+template <typename T, int LDS, int NRHS, int NP>
+__device__ __forceinline__ void residual_blk(T* S, const double* phi, const double* pm,
+                                             const double* x64, const double* b64, int ks,
+                                             int lane) {
+    const int n = NP + ks;
+    for (int r = lane; r < n; r += 32) {
+        double acc[NRHS];
+#pragma unroll
+        for (int q = 0; q < NRHS; ++q) acc[q] = b64[r * NRHS + q];
+        if (r < NP) {
+            for (int j = 0; j < ks; ++j) {
+                const double mv = pm[j * NP + r];
+#pragma unroll
+                for (int q = 0; q < NRHS; ++q) acc[q] = fma(-mv, x64[(NP + j) * NRHS + q], acc[q]);
+            }
+        } else {
+            const int i = r - NP;
+#pragma unroll
+            for (int m = 0; m < NP; ++m) {
+                const double mv = pm[i * NP + m];
+#pragma unroll
+                for (int q = 0; q < NRHS; ++q) acc[q] = fma(-mv, x64[m * NRHS + q], acc[q]);
+            }
+            // phi(i, j) for j < i: column i of the packed upper triangle,
+            // tri(j, i) advancing by ks - j - 2; for j > i: row i, contiguous
+            int t = i - 1;  // tri(0, i)
+            for (int j = 0; j < i; ++j) {
+                const double fv = phi[t];
+                t += ks - j - 2;
+#pragma unroll
+                for (int q = 0; q < NRHS; ++q) acc[q] = fma(-fv, x64[(NP + j) * NRHS + q], acc[q]);
+            }
+            const double* prow_i = phi + (i < ks - 1 ? tri_idx(i, i + 1, ks) : 0);
+            for (int j = i + 1; j < ks; ++j) {
+                const double fv = prow_i[j - i - 1];
+#pragma unroll
+                for (int q = 0; q < NRHS; ++q) acc[q] = fma(-fv, x64[(NP + j) * NRHS + q], acc[q]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < NRHS; ++q) S[r * LDS + n + q] = static_cast<T>(acc[q]);
+    }
+    __syncwarp();
+}
+
 // Scatter of the k node weights (unknowns NP .. NP+ks-1), rescaled,
 // src/rbf_operators.h:368-375; NaN for a singular stencil; info.
 template <typename T, int NRHS>
@@ -476,6 +604,10 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
     int* nja = reinterpret_cast<int*>(smem + C::off_nja);
     double* nxy = reinterpret_cast<double*>(smem + C::off_nxy);
     int* nia = reinterpret_cast<int*>(smem + C::off_nia);
+    double* phi = MIXED ? reinterpret_cast<double*>(smem + C::off_phi) : nullptr;
+    double* pm = MIXED ? reinterpret_cast<double*>(smem + C::off_pm) : nullptr;
+    double* x64 = MIXED ? reinterpret_cast<double*>(smem + C::off_x64) : nullptr;
+    double* b64 = MIXED ? reinterpret_cast<double*>(smem + C::off_b64) : nullptr;
 
     // With PF, stencil s was prefetched (by the previous call of this warp, or
     // by prefetch_first): its neighbour coordinates wait in cx/cy (raw), its
@@ -507,7 +639,7 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
         }
     }
     const int e = gather_scale<C::KMAX, PF>(p, off, ks, x0, y0, cx, cy, lane);
-    fill_system<T, LDS, NRHS, P, Q>(p, S, cx, cy, ks, e, alive, NMAX, lane);
+    fill_system<T, LDS, NRHS, P, Q>(p, S, cx, cy, ks, e, alive, NMAX, lane, phi, pm, b64);
 
     // prefetch stage 2: the next stencil's ja row (its bounds have landed)
     if constexpr (PF) {
@@ -541,7 +673,77 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
         }
     }
     back_substitute_blk<T, R, LDS, NRHS>(S, pinv, piv, X, n, lane);
-    scatter_blk<T, NRHS>(p, X, NP, ks, off, e, info, s, lane);
+    if constexpr (!MIXED) {
+        scatter_blk<T, NRHS>(p, X, NP, ks, off, e, info, s, lane);
+    } else {
+        // ---- FP64 iterative refinement with the FP32 factors
+        for (int i = lane; i < n * NRHS; i += G) x64[i] = static_cast<double>(X[i]);
+        __syncwarp();
+        int sweeps = 0;
+        bool converged = false, failed = (info != 0);
+        float prev = 3.4e38f;
+        while (!converged && !failed) {
+            if (sweeps >= p.max_sweeps) {
+                failed = true;
+                break;
+            }
+            ++sweeps;
+            residual_blk<T, LDS, NRHS, NP>(S, phi, pm, x64, b64, ks, lane);
+            forward_substitute_blk<T, R, LDS, NRHS>(S, piv, n, lane);
+            back_substitute_blk<T, R, LDS, NRHS>(S, pinv, piv, X, n, lane);
+            // x += d; convergence on max|d| / max|x| per right-hand side
+            float worst = 0.f;
+            for (int q = 0; q < p.nrhs; ++q) {
+                float dmax = 0.f, xmax = 0.f;
+                for (int i = lane; i < n; i += G) {
+                    const double d = static_cast<double>(X[i * NRHS + q]);
+                    const double xn = x64[i * NRHS + q] + d;
+                    x64[i * NRHS + q] = xn;
+                    dmax = fmaxf(dmax, (float)fabs(d));
+                    xmax = fmaxf(xmax, (float)fabs(xn));
+                }
+                dmax = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(dmax)));
+                xmax = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(xmax)));
+                worst = fmaxf(worst, xmax > 0.f ? dmax / xmax : dmax);
+            }
+            __syncwarp();
+            // The correction of sweep k measures the error before it (tau_k);
+            // the error left after it is about tau_k * rho / (1 - rho) with
+            // rho = tau_k / tau_(k-1) the observed contraction (about
+            // cond(M) * 2^-24). Converged when that prediction is below tol
+            // (or the correction itself is at the FP64 floor). A contraction
+            // above 0.1 means cond(M) > ~1e6: the prediction is unreliable
+            // there and the FP64 rounding floor of the system itself nears the
+            // tolerance, so such a stencil (and a NaN) goes to the FP64 kernel.
+            if (!(worst == worst)) {
+                failed = true;
+            } else {
+                const float rho = sweeps >= 2 ? worst / fmaxf(prev, 1e-38f) : 1.0f;
+                const float left = rho < 0.1f ? worst * rho / (1.0f - rho) : worst;
+                if (left <= (float)p.ir_tol || worst <= 1e-15f) converged = true;
+                else if (sweeps >= 2 && rho > 0.1f) failed = true;
+            }
+            prev = worst;
+        }
+        if (lane == 0) {
+            if (p.sweeps_sum) atomicAdd(p.sweeps_sum, (unsigned long long)sweeps);
+            if (p.sweeps_max) atomicMax(p.sweeps_max, sweeps);
+        }
+        if (failed) {
+            if (lane == 0) {
+                const int fo = p.list_off_dev ? *p.list_off_dev : 0;
+                p.fb_list[fo + atomicAdd(p.fb_count, 1)] = s;
+            }
+        } else {
+            for (int q = 0; q < p.nrhs; ++q) {
+                double* dst = out_column(p, q) + off;
+                const int sh = -op_order(p.col_op[q]) * e;
+                for (int j = lane; j < ks; j += G) dst[j] = scalbn(x64[(NP + j) * NRHS + q], sh);
+            }
+            if (lane == 0 && p.info) p.info[s - p.row_base] = 0;
+        }
+        __syncwarp();
+    }
 }
 
 template <typename T, int NMAX, int NRHS, int P, int Q, bool MIXED, int BLOCK, int MINB, int PB,

@@ -35,3 +35,6 @@ RBFB_BLK_VARIANT(b64_p4q7_n64_pb8, double, 64, 3, 4, 7, false, 32, 1, 8, true)
 RBFB_BLK_VARIANT(b64_p4q7_n80_pb8, double, 80, 3, 4, 7, false, 32, 1, 8, true)
 RBFB_BLK_VARIANT(b64_p3q5_n45_pb8, double, 45, 3, 3, 5, false, 96, 1, 8, true)
 RBFB_BLK_VARIANT(b64_p3q5_n45_pb16, double, 45, 3, 3, 5, false, 96, 1, 16, true)
+RBFB_BLK_VARIANT(bmx_p3q5_n45_pb8, float, 45, 3, 3, 5, true, 96, 1, 8, true)
+RBFB_BLK_VARIANT(bmx_p2q3_n32_pb8, float, 32, 3, 2, 3, true, 128, 1, 8, true)
+RBFB_BLK_VARIANT(bmx_p4q7_n80_pb8, float, 80, 3, 4, 7, true, 32, 1, 8, true)
