@@ -2,19 +2,24 @@
 // (feq_kernel, macros_kernel, bgk_kernel_split: src/lbm/d2q9_kernels.cu and
 // its header), for both instantiations.
 //
-// TEST INFRASTRUCTURE. oracle/Makefile compiles this file together with the
-// reference's d2q9_kernels.cu where it lies (nothing of it is copied here)
-// into oracle/_ref/libref_lbm.so, with --fmad=false so that every product and
+// TEST INFRASTRUCTURE. oracle/Makefile compiles this file, which includes the
+// reference's d2q9_kernels.cu where it lies (nothing of it is copied here;
+// one translation unit, so the kernel templates and their launches meet),
+// into oracle/_ref/libref_lbm.so with --fmad=false, so that every product and
 // sum is rounded as the source writes it. Only the GPU tests load it: it pins
 // the library's LBM kernels to the reference's own, bit for bit. The
-// launchers take device pointers and synchronise; they allocate nothing.
+// launchers take device pointers, check the launch and synchronise; they
+// allocate nothing. They return 0, or -1 (launch error) / -2 (run error).
 #include <cuda_runtime.h>
 
-#include "d2q9_kernels.h"
+#include "d2q9_kernels.cu"
 
 namespace {
 inline int grid(int n) { return (n + 255) / 256; }
-inline int done() { return cudaDeviceSynchronize() == cudaSuccess ? 0 : -1; }
+inline int done() {
+    if (cudaGetLastError() != cudaSuccess) return -1;
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : -2;
+}
 }  // namespace
 
 extern "C" {
