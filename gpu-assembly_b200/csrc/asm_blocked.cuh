@@ -5,8 +5,10 @@
 // Replaces assemble_interp_weights<Config> (src/rbf_operators.h:292-376),
 // whose solve is cuSolverDx gesv_partial_pivot with one stencil per CTA.
 //
-// One warp owns one stencil; a CTA holds BLOCK / 32 warps and the grid is
-// persistent. The system is not padded: n = npoly(P) + k_s unknowns for the
+// A group of G lanes owns one stencil: a warp (G = 32) or a half warp (G =
+// 16, two stencils per warp, each step's shuffles and reductions over the
+// half's lanes only, so the per-step instruction overhead is paid once for
+// two stencils). A CTA holds BLOCK / G groups and the grid is persistent. The system is not padded: n = npoly(P) + k_s unknowns for the
 // stencil's own k_s, any n <= NMAX. It is stored row-major in S (row =
 // equation, column = unknown) with the NRHS right-hand sides as columns
 // n .. n+NRHS-1, polynomial block first: equations [P^T rows (NP), node rows
@@ -15,13 +17,13 @@
 //
 // The elimination runs in panels of PB columns. For panel [c0, c0+PB):
 //   1. the rows not yet pivoted are listed in ascending order (act[]); lane
-//      l takes list positions l, l+32, ... and loads their PB panel columns
+//      l takes list positions l, l+G, ... and loads their PB panel columns
 //      into registers;
 //   2. PB steps on the panel columns only. Step c: pivot = the unused row of
 //      largest key (a 32-bit key: the magnitude word of a(r,c) without its 7
 //      lowest bits, plus one, with 127 - list position in those bits, so ties
 //      go to the lowest row -- the oracle's rule), found by one warp
-//      reduction whose operands were formed at the end of the previous step;
+//      group reduction whose operands were formed at the end of the previous step;
 //      the pivot row's owner writes its whole panel row to S (final: L
 //      multipliers left of c, the pivot, U right of it) and 1 / pivot (rounded
 //      once, the oracle's reciprocal); every other unused row takes
@@ -33,13 +35,13 @@
 //      included): row p_t takes the updates of steps t' < t, in order;
 //   5. every unused row over the trailing columns: the PB updates of the
 //      panel, in order, multipliers from registers, pivot-row values read
-//      once per column pair and broadcast to the warp.
+//      once per column pair and broadcast to the group.
 // Every matrix and right-hand-side element receives exactly the fused
 // multiply-adds of the unblocked elimination, in the same order, so the FP64
 // result is bit-identical to the oracle's.
 //
 // Back substitution is column oriented, as the oracle's: lane l holds the
-// transformed right-hand sides of the rows pivoted at steps l, l+32, ...;
+// transformed right-hand sides of the rows pivoted at steps l, l+G, ...;
 // for c = n-1 .. 0 the owner of step c forms x_c = y * (1 / pivot_c) and
 // broadcasts it by shuffle, and the rows pivoted before c update with
 // u(row, c).
@@ -53,14 +55,16 @@ namespace rbfb {
 
 // Layout of one stencil's working set for systems of up to NMAX unknowns
 // with up to KMAX neighbours (shared memory, or a global scratch region).
-template <typename T, int NMAX, int NRHS, int KMAX_, int PB>
+template <typename T, int NMAX, int NRHS, int KMAX_, int PB, int G_ = 32>
 struct BlkLayout {
-    static constexpr int G = 32;  // lanes per stencil: one warp
+    static constexpr int G = G_;  // lanes per stencil: a warp, or half of one
     static constexpr int KMAX = KMAX_;
     static constexpr int R = (NMAX + G - 1) / G;  // list positions per lane
     static constexpr int VE = 16 / (int)sizeof(T);  // elements per 16-byte vector
     static_assert(PB % VE == 0, "panels are whole vectors");
     static_assert(NMAX <= 128, "pivot keys carry the list position in 7 bits");
+    static_assert(G == 32 || G == 16, "a stencil takes a warp or a half warp");
+    static_assert(R <= 4, "the substitutions walk at most four step segments");
     static constexpr int WMAX = NMAX + NRHS;  // columns: unknowns + right-hand sides
     // Row stride in vectors: odd, so the 32 rows a warp reads down one column
     // fall in different bank groups (4 wavefronts for 32 vectors).
@@ -85,9 +89,9 @@ struct BlkLayout {
     static constexpr int bytes = off_nia + 16;
 };
 
-template <typename T, int NMAX, int NRHS, int P, int Q, bool MIXED, int PB>
-struct BlkCfg : BlkLayout<T, NMAX, NRHS, NMAX - npoly(P), PB> {
-    using L = BlkLayout<T, NMAX, NRHS, NMAX - npoly(P), PB>;
+template <typename T, int NMAX, int NRHS, int P, int Q, bool MIXED, int PB, int G_ = 32>
+struct BlkCfg : BlkLayout<T, NMAX, NRHS, NMAX - npoly(P), PB, G_> {
+    using L = BlkLayout<T, NMAX, NRHS, NMAX - npoly(P), PB, G_>;
     static_assert(MIXED ? sizeof(T) == 4 : sizeof(T) == 8,
                   "FP64 factors for the plain form, FP32 factors for the refined one");
     static constexpr int NP = npoly(P);
@@ -138,10 +142,10 @@ __device__ __forceinline__ uint32_t hiword(float v) { return __float_as_uint(v);
 // power-of-two radius scale (src/rbf_operators.h:354-358): cx/cy receive the
 // shifted, scaled coordinates of the ks neighbours (with PF they hold the
 // raw prefetched ones on entry). Returns the scale exponent e.
-template <int KMAX, bool PF>
+template <int KMAX, bool PF, int G = 32>
 __device__ __forceinline__ int gather_scale(const AsmParams& p, int off, int ks, double x0,
                                             double y0, double* cx, double* cy, int lane) {
-    constexpr int G = 32, KPL = (KMAX + G - 1) / G;
+    constexpr int KPL = (KMAX + G - 1) / G;
     double gx[KPL], gy[KPL];
     int emax = -100000;
 #pragma unroll
@@ -165,7 +169,7 @@ __device__ __forceinline__ int gather_scale(const AsmParams& p, int off, int ks,
             if (gy[t] != 0.0) emax = max(emax, ilogb(fabs(gy[t])) + 1);
         }
     }
-    int e = __reduce_max_sync(0xffffffffu, emax);
+    int e = __reduce_max_sync(group_mask(G), emax);
     e = (p.scale && e > -100000) ? e : 0;
 #pragma unroll
     for (int t = 0; t < KPL; ++t) {
@@ -175,7 +179,7 @@ __device__ __forceinline__ int gather_scale(const AsmParams& p, int off, int ks,
             cy[j] = scalbn(gy[t], -e);
         }
     }
-    __syncwarp();
+    __syncwarp(group_mask(G));
     return e;
 }
 
@@ -186,13 +190,13 @@ __device__ __forceinline__ int gather_scale(const AsmParams& p, int off, int ks,
 // With phi != nullptr (the refined form) the FP64 values are also kept: phi
 // (pair (i, j), i < j, at its number in row-major order of the strict upper
 // triangle), pm[i*NP + m] (monomials of node i) and b64[r*NRHS + q].
-template <typename T, int LDS, int NRHS, int P, int Q>
+template <typename T, int LDS, int NRHS, int P, int Q, int G = 32>
 __device__ __forceinline__ void fill_system(const AsmParams& p, T* S, const double* cx,
                                             const double* cy, int ks, int e,
                                             unsigned char* alive, int nmax, int lane,
                                             double* phi = nullptr, double* pm = nullptr,
                                             double* b64 = nullptr) {
-    constexpr int G = 32, NP = npoly(P);
+    constexpr int NP = npoly(P);
     const int n = NP + ks;
     {
         const int npair = ks * (ks - 1) / 2;
@@ -250,11 +254,12 @@ __device__ __forceinline__ void fill_system(const AsmParams& p, T* S, const doub
 // Blocked right-looking elimination of the n x n system in S with its NRHS
 // right-hand-side columns (panels of PB; R list positions per lane, R*32 >=
 // n). Returns info: 0, or c + 1 for the first zero pivot.
-template <typename T, int R, int LDS, int NRHS, int PB>
+template <typename T, int R, int LDS, int NRHS, int PB, int G = 32>
 __device__ __forceinline__ int eliminate_blocked(T* S, T* pinv, int* piv, int* act,
                                                  unsigned char* alive, int n, int lane) {
-    constexpr int G = 32, VE = 16 / (int)sizeof(T);
-    constexpr unsigned FULL = 0xffffffffu;
+    constexpr int VE = 16 / (int)sizeof(T);
+    const unsigned FULL = group_mask(G);  // the group's lanes
+    const int gbase = (threadIdx.x & 31) & ~(G - 1);
     const int W = n + NRHS;  // columns in use
     int info = 0;
 #pragma unroll 1
@@ -265,11 +270,11 @@ __device__ __forceinline__ int eliminate_blocked(T* S, T* pinv, int* piv, int* a
         for (int j = 0; j < R; ++j) {
             const int r = lane + G * j;
             const bool a = r < n && alive[r];
-            const unsigned b = __ballot_sync(FULL, a);
+            const unsigned b = (__ballot_sync(FULL, a) & FULL) >> gbase;
             if (a) act[m + __popc(b & ((1u << lane) - 1u))] = r;
             m += __popc(b);
         }
-        __syncwarp();
+        __syncwarp(group_mask(G));
         T a[R][PB];
         int arow[R];
         uint32_t kmask[R], kcon[R];
@@ -327,7 +332,7 @@ __device__ __forceinline__ int eliminate_blocked(T* S, T* pinv, int* piv, int* a
                     }
                     pinv[c] = pinvl;
                 }
-                __syncwarp();
+                __syncwarp(group_mask(G));
                 const T inv = pinv[c];
                 const T* U = S + piv[c] * LDS + c0;
                 // multipliers of the unused rows (0 for the others)
@@ -359,7 +364,7 @@ __device__ __forceinline__ int eliminate_blocked(T* S, T* pinv, int* piv, int* a
                 for (int v4 = 0; v4 < PB; v4 += VE) stv(dst + v4, &a[sl][v4]);
             }
         }
-        __syncwarp();
+        __syncwarp(group_mask(G));
         const int jt = c0 + PB;  // first trailing column
         if (jt >= W) break;
         const int nv = (W - jt + VE - 1) / VE;  // trailing column vectors
@@ -384,7 +389,7 @@ __device__ __forceinline__ int eliminate_blocked(T* S, T* pinv, int* piv, int* a
                 }
             }
         }
-        __syncwarp();
+        __syncwarp(group_mask(G));
         // 5. the unused rows over the trailing columns (all lanes walk the same
         // columns: the pivot-row values are broadcast loads)
         if (m > tend) {
@@ -411,22 +416,21 @@ __device__ __forceinline__ int eliminate_blocked(T* S, T* pinv, int* piv, int* a
                     }
                 }
             }
-            __syncwarp();
+            __syncwarp(group_mask(G));
         }
     }
     return info;
 }
 
 // Column-oriented back substitution (the oracle's order): lane l holds the
-// transformed right-hand sides of the rows pivoted at steps l, l + 32, ...;
+// transformed right-hand sides of the rows pivoted at steps l, l + G, ...;
 // for c = n-1 .. 0 the owner of step c forms x_c = y * (1 / pivot_c) and
 // broadcasts it by shuffle, and the rows pivoted before c update with
 // u(row, c). X[c*NRHS + q] receives x_c.
-template <typename T, int R, int LDS, int NRHS>
+template <typename T, int R, int LDS, int NRHS, int G = 32>
 __device__ __forceinline__ void back_substitute_blk(const T* S, const T* pinv, const int* piv,
                                                     T* X, int n, int lane) {
-    constexpr int G = 32;
-    constexpr unsigned FULL = 0xffffffffu;
+    const unsigned FULL = group_mask(G);
     T y[R][NRHS];
     int prow_t[R];
 #pragma unroll
@@ -436,7 +440,7 @@ __device__ __forceinline__ void back_substitute_blk(const T* S, const T* pinv, c
 #pragma unroll
         for (int q = 0; q < NRHS; ++q) y[sl][q] = t < n ? S[prow_t[sl] * LDS + n + q] : T(0);
     }
-    // Steps in segments of 32 from the last: in segment OS the owner of step c
+    // Steps in segments of G from the last: in segment OS the owner of step c
     // holds it in slot OS (static), the slots below OS hold steps all before
     // c (updated unconditionally), the slots above OS steps all after it.
     auto segment = [&](auto os_c) {
@@ -446,7 +450,7 @@ __device__ __forceinline__ void back_substitute_blk(const T* S, const T* pinv, c
             const T dv = pinv[c];
             T xq[NRHS];
 #pragma unroll
-            for (int q = 0; q < NRHS; ++q) xq[q] = __shfl_sync(FULL, y[OS][q] * dv, c - G * OS);
+            for (int q = 0; q < NRHS; ++q) xq[q] = __shfl_sync(FULL, y[OS][q] * dv, c - G * OS, G);
             if (lane == 0) {
 #pragma unroll
                 for (int q = 0; q < NRHS; ++q) X[c * NRHS + q] = xq[q];
@@ -464,19 +468,18 @@ __device__ __forceinline__ void back_substitute_blk(const T* S, const T* pinv, c
     if constexpr (R > 2) segment(std::integral_constant<int, 2>{});
     if constexpr (R > 1) segment(std::integral_constant<int, 1>{});
     segment(std::integral_constant<int, 0>{});
-    __syncwarp();
+    __syncwarp(group_mask(G));
 }
 
 // Forward substitution with the unit lower factor kept in S (the refined
 // form): the right-hand sides in S's columns n .. n+NRHS-1, in row order, are
 // replaced by L^-1 P b in the layout the elimination leaves them (row piv[t]
-// holds component t). Lane l holds the components of steps l, l + 32, ...;
+// holds component t). Lane l holds the components of steps l, l + G, ...;
 // for c = 0 .. n-1 the owner of step c broadcasts it by shuffle and the rows
 // pivoted after c update with their multiplier l(row, c) = S(row, c).
-template <typename T, int R, int LDS, int NRHS>
+template <typename T, int R, int LDS, int NRHS, int G = 32>
 __device__ __forceinline__ void forward_substitute_blk(T* S, const int* piv, int n, int lane) {
-    constexpr int G = 32;
-    constexpr unsigned FULL = 0xffffffffu;
+    const unsigned FULL = group_mask(G);
     T y[R][NRHS];
     int prow_t[R];
 #pragma unroll
@@ -486,7 +489,7 @@ __device__ __forceinline__ void forward_substitute_blk(T* S, const int* piv, int
 #pragma unroll
         for (int q = 0; q < NRHS; ++q) y[sl][q] = t < n ? S[prow_t[sl] * LDS + n + q] : T(0);
     }
-    // segments of 32 steps from the first: in segment OS the owner of step c
+    // segments of G steps from the first: in segment OS the owner of step c
     // holds it in slot OS, the slots above OS hold steps all after c
     auto segment = [&](auto os_c) {
         constexpr int OS = decltype(os_c)::value;
@@ -494,7 +497,7 @@ __device__ __forceinline__ void forward_substitute_blk(T* S, const int* piv, int
         for (int c = G * OS; c < min(n, G * (OS + 1)); ++c) {
             T z[NRHS];
 #pragma unroll
-            for (int q = 0; q < NRHS; ++q) z[q] = __shfl_sync(FULL, y[OS][q], c - G * OS);
+            for (int q = 0; q < NRHS; ++q) z[q] = __shfl_sync(FULL, y[OS][q], c - G * OS, G);
 #pragma unroll
             for (int sl = OS; sl < R; ++sl) {
                 T l = S[prow_t[sl] * LDS + c];
@@ -515,7 +518,7 @@ __device__ __forceinline__ void forward_substitute_blk(T* S, const int* piv, int
             for (int q = 0; q < NRHS; ++q) S[prow_t[sl] * LDS + n + q] = y[sl][q];
         }
     }
-    __syncwarp();
+    __syncwarp(group_mask(G));
 }
 
 // Packed index of the pair (i, j), i < j, of a k-node stencil.
@@ -525,12 +528,12 @@ __device__ __forceinline__ int tri_idx(int i, int j, int k) {
 
 // FP64 residual b - M x of the refined form, from the FP64 copies, rounded to
 // T into S's right-hand-side columns (row order).
-template <typename T, int LDS, int NRHS, int NP>
+template <typename T, int LDS, int NRHS, int NP, int G = 32>
 __device__ __forceinline__ void residual_blk(T* S, const double* phi, const double* pm,
                                              const double* x64, const double* b64, int ks,
                                              int lane) {
     const int n = NP + ks;
-    for (int r = lane; r < n; r += 32) {
+    for (int r = lane; r < n; r += G) {
         double acc[NRHS];
 #pragma unroll
         for (int q = 0; q < NRHS; ++q) acc[q] = b64[r * NRHS + q];
@@ -567,31 +570,31 @@ __device__ __forceinline__ void residual_blk(T* S, const double* phi, const doub
 #pragma unroll
         for (int q = 0; q < NRHS; ++q) S[r * LDS + n + q] = static_cast<T>(acc[q]);
     }
-    __syncwarp();
+    __syncwarp(group_mask(G));
 }
 
 // Scatter of the k node weights (unknowns NP .. NP+ks-1), rescaled,
 // src/rbf_operators.h:368-375; NaN for a singular stencil; info.
-template <typename T, int NRHS>
+template <typename T, int NRHS, int G = 32>
 __device__ __forceinline__ void scatter_blk(const AsmParams& p, const T* X, int np, int ks, int off,
                                             int e, int info, int s, int lane) {
     const bool bad = info != 0;
     for (int q = 0; q < p.nrhs; ++q) {
         double* dst = out_column(p, q) + off;
         const int sh = -op_order(p.col_op[q]) * e;
-        for (int j = lane; j < ks; j += 32) {
+        for (int j = lane; j < ks; j += G) {
             const double v = static_cast<double>(X[(np + j) * NRHS + q]);
             dst[j] = bad ? __longlong_as_double(0x7ff8000000000000ll) : scalbn(v, sh);
         }
     }
     if (lane == 0 && p.info) p.info[s - p.row_base] = info;
-    __syncwarp();
+    __syncwarp(group_mask(G));
 }
 
-template <typename T, int NMAX, int NRHS, int P, int Q, bool MIXED, int PB, bool PF>
+template <typename T, int NMAX, int NRHS, int P, int Q, bool MIXED, int PB, bool PF, int GW = 32>
 __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, char* smem,
                                              int lane) {
-    using C = BlkCfg<T, NMAX, NRHS, P, Q, MIXED, PB>;
+    using C = BlkCfg<T, NMAX, NRHS, P, Q, MIXED, PB, GW>;
     constexpr int G = C::G, NP = C::NP, R = C::R, LDS = C::LDS;
     double* cx = reinterpret_cast<double*>(smem + C::off_cx);
     double* cy = reinterpret_cast<double*>(smem + C::off_cy);
@@ -617,12 +620,12 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
     double x0, y0;
     if constexpr (PF) {
         cp_async_wait_all();
-        __syncwarp();
+        __syncwarp(group_mask(G));
         x0 = nxy[0];
         y0 = nxy[1];
         off = p.ia ? nia[0] : (s - p.row_base) * p.k;
         ks = p.ia ? nia[1] - off : p.k;
-        __syncwarp();  // read before the slots are refilled below
+        __syncwarp(group_mask(G));  // read before the slots are refilled below
     } else {
         x0 = p.x[s];
         y0 = p.y[s];
@@ -638,8 +641,8 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
             cp_async4(nia + 1, p.ia + sn + 1);
         }
     }
-    const int e = gather_scale<C::KMAX, PF>(p, off, ks, x0, y0, cx, cy, lane);
-    fill_system<T, LDS, NRHS, P, Q>(p, S, cx, cy, ks, e, alive, NMAX, lane, phi, pm, b64);
+    const int e = gather_scale<C::KMAX, PF, G>(p, off, ks, x0, y0, cx, cy, lane);
+    fill_system<T, LDS, NRHS, P, Q, G>(p, S, cx, cy, ks, e, alive, NMAX, lane, phi, pm, b64);
 
     // prefetch stage 2: the next stencil's ja row (its bounds have landed)
     if constexpr (PF) {
@@ -647,7 +650,7 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
         if (sn >= 0) {
             if (p.ia) {
                 cp_async_wait_all();
-                __syncwarp();
+                __syncwarp(group_mask(G));
                 offn = nia[0];
                 ksn = nia[1] - offn;
             } else {
@@ -656,12 +659,12 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
             }
             for (int j = lane; j < ksn; j += G) cp_async4(nja + j, p.ja + offn + j);
         }
-        __syncwarp();
+        __syncwarp(group_mask(G));
         if (lane == 0) nia[2] = ksn;
     }
-    __syncwarp();
+    __syncwarp(group_mask(G));
 
-    const int info = eliminate_blocked<T, R, LDS, NRHS, PB>(S, pinv, piv, act, alive, n, lane);
+    const int info = eliminate_blocked<T, R, LDS, NRHS, PB, G>(S, pinv, piv, act, alive, n, lane);
 
     // prefetch stage 3: the next stencil's neighbour coordinates into cx/cy
     if (const int ksn = PF ? nia[2] : 0; ksn > 0) {
@@ -672,13 +675,13 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
             cp_async8(cy + j, p.y + nb);
         }
     }
-    back_substitute_blk<T, R, LDS, NRHS>(S, pinv, piv, X, n, lane);
+    back_substitute_blk<T, R, LDS, NRHS, G>(S, pinv, piv, X, n, lane);
     if constexpr (!MIXED) {
-        scatter_blk<T, NRHS>(p, X, NP, ks, off, e, info, s, lane);
+        scatter_blk<T, NRHS, G>(p, X, NP, ks, off, e, info, s, lane);
     } else {
         // ---- FP64 iterative refinement with the FP32 factors
         for (int i = lane; i < n * NRHS; i += G) x64[i] = static_cast<double>(X[i]);
-        __syncwarp();
+        __syncwarp(group_mask(G));
         int sweeps = 0;
         bool converged = false, failed = (info != 0);
         float prev = 3.4e38f;
@@ -688,9 +691,9 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
                 break;
             }
             ++sweeps;
-            residual_blk<T, LDS, NRHS, NP>(S, phi, pm, x64, b64, ks, lane);
-            forward_substitute_blk<T, R, LDS, NRHS>(S, piv, n, lane);
-            back_substitute_blk<T, R, LDS, NRHS>(S, pinv, piv, X, n, lane);
+            residual_blk<T, LDS, NRHS, NP, G>(S, phi, pm, x64, b64, ks, lane);
+            forward_substitute_blk<T, R, LDS, NRHS, G>(S, piv, n, lane);
+            back_substitute_blk<T, R, LDS, NRHS, G>(S, pinv, piv, X, n, lane);
             // x += d; convergence on max|d| / max|x| per right-hand side
             float worst = 0.f;
             for (int q = 0; q < p.nrhs; ++q) {
@@ -702,11 +705,11 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
                     dmax = fmaxf(dmax, (float)fabs(d));
                     xmax = fmaxf(xmax, (float)fabs(xn));
                 }
-                dmax = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(dmax)));
-                xmax = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(xmax)));
+                dmax = __uint_as_float(__reduce_max_sync(group_mask(G), __float_as_uint(dmax)));
+                xmax = __uint_as_float(__reduce_max_sync(group_mask(G), __float_as_uint(xmax)));
                 worst = fmaxf(worst, xmax > 0.f ? dmax / xmax : dmax);
             }
-            __syncwarp();
+            __syncwarp(group_mask(G));
             // The correction of sweep k measures the error before it (tau_k);
             // the error left after it is about tau_k * rho / (1 - rho) with
             // rho = tau_k / tau_(k-1) the observed contraction (about
@@ -742,15 +745,16 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
             }
             if (lane == 0 && p.info) p.info[s - p.row_base] = 0;
         }
-        __syncwarp();
+        __syncwarp(group_mask(G));
     }
 }
 
 template <typename T, int NMAX, int NRHS, int P, int Q, bool MIXED, int BLOCK, int MINB, int PB,
-          bool PF>
+          bool PF, int GW = 32>
 __global__ void __launch_bounds__(BLOCK, MINB) blk_kernel(AsmParams p) {
-    using C = BlkCfg<T, NMAX, NRHS, P, Q, MIXED, PB>;
+    using C = BlkCfg<T, NMAX, NRHS, P, Q, MIXED, PB, GW>;
     constexpr int G = C::G;
+    const unsigned gmask = group_mask(G);
     constexpr int GPB = BLOCK / G;  // warps (stencils in flight) per CTA
     extern __shared__ __align__(16) char smem_raw[];
     const int gib = threadIdx.x / G;
@@ -763,7 +767,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) blk_kernel(AsmParams p) {
         if (!p.work) return next_static;
         int v = 0;
         if (lane == 0) v = atomicAdd(p.work, 1);
-        return __shfl_sync(0xffffffffu, v, 0);
+        return __shfl_sync(gmask, v, 0, G);
     };
     auto item = [&](int i) { return i < n ? (list ? list[i] : p.item_base + i) : -1; };
     // One call site: the stencil body is inlined once. With PF each call
@@ -771,14 +775,15 @@ __global__ void __launch_bounds__(BLOCK, MINB) blk_kernel(AsmParams p) {
     int* next_it = reinterpret_cast<int*>(smem + C::off_nia) + 3;
     int it = claim(blockIdx.x * GPB + gib);
     if constexpr (PF) {
-        if (it < n) prefetch_first<C>(p, item(it), smem, lane, 0xffffffffu);
+        if (it < n) prefetch_first<C>(p, item(it), smem, lane, gmask);
     }
     while (it < n) {
         const int itn = claim(it + ngroups);
         if (lane == 0) *next_it = itn;
-        assemble_blk<T, NMAX, NRHS, P, Q, MIXED, PB, PF>(p, item(it), PF ? item(itn) : -1, smem, lane);
+        assemble_blk<T, NMAX, NRHS, P, Q, MIXED, PB, PF, GW>(p, item(it), PF ? item(itn) : -1, smem,
+                                                             lane);
         it = *next_it;
-        __syncwarp();
+        __syncwarp(group_mask(G));
     }
 }
 
@@ -812,7 +817,7 @@ __device__ __forceinline__ void fill_system_q(const AsmParams& p, int Q, T* S, c
 template <typename T, class L, int NRHS, int PB>
 __device__ __forceinline__ void assemble_any(const AsmParams& p, int s, int off, int ks, int P,
                                              int Q, char* base, int lane) {
-    constexpr int LDS = L::LDS;
+    constexpr int LDS = L::LDS, G = L::G;
     double* cx = reinterpret_cast<double*>(base + L::off_cx);
     double* cy = reinterpret_cast<double*>(base + L::off_cy);
     T* S = reinterpret_cast<T*>(base + L::off_s);
@@ -829,7 +834,7 @@ __device__ __forceinline__ void assemble_any(const AsmParams& p, int s, int off,
         case 3: fill_system_q<T, LDS, NRHS, 3>(p, Q, S, cx, cy, ks, e, alive, n, lane); break;
         default: fill_system_q<T, LDS, NRHS, 4>(p, Q, S, cx, cy, ks, e, alive, n, lane); break;
     }
-    __syncwarp();
+    __syncwarp(group_mask(G));
     const int info = eliminate_blocked<T, L::R, LDS, NRHS, PB>(S, pinv, piv, act, alive, n, lane);
     back_substitute_blk<T, L::R, LDS, NRHS>(S, pinv, piv, X, n, lane);
     scatter_blk<T, NRHS>(p, X, np, ks, off, e, info, s, lane);
@@ -846,7 +851,7 @@ template <typename T, int NS, int NG, int NRHS, int BLOCK, int PB>
 __global__ void __launch_bounds__(BLOCK, 1)
     blk_csr_kernel(AsmParams p, const int8_t* degree, int P0, int phs, char* gscratch, int* err) {
     using C = CsrCfg<T, NS, NG, NRHS, PB>;
-    constexpr int GPB = BLOCK / 32;
+    constexpr int G = 32, GPB = BLOCK / G;
     extern __shared__ __align__(16) char smem_raw[];
     const int gib = threadIdx.x / 32;
     const int lane = threadIdx.x % 32;

@@ -14,7 +14,8 @@
 //
 // RBFB_BLK_VARIANT(name, T, NMAX, NRHS, P, Q, MIXED, BLOCK, MINB, PB, PF): the
 // blocked shared-memory kernel (asm_blocked.cuh), one warp per stencil, any
-// system size n <= NMAX, panels of PB columns.
+// system size n <= NMAX, panels of PB columns. RBFB_BLK16_VARIANT: the same
+// with half-warp groups, two stencils per warp.
 // The build compiles each line as its own translation unit.
 RBFB_VARIANT(f64_p2q3_n32_g16x2, double, 16, 2, 32, 3, 2, 3, false, 64, 6, false, true)
 RBFB_VARIANT(f64_p2q3_n32_g16x1, double, 16, 1, 32, 3, 2, 3, false, 64, 1, false, true)
@@ -38,3 +39,5 @@ RBFB_BLK_VARIANT(b64_p3q5_n45_pb16, double, 45, 3, 3, 5, false, 96, 1, 16, true)
 RBFB_BLK_VARIANT(bmx_p3q5_n45_pb8, float, 45, 3, 3, 5, true, 96, 1, 8, true)
 RBFB_BLK_VARIANT(bmx_p2q3_n32_pb8, float, 32, 3, 2, 3, true, 128, 1, 8, true)
 RBFB_BLK_VARIANT(bmx_p4q7_n80_pb8, float, 80, 3, 4, 7, true, 32, 1, 8, true)
+RBFB_BLK16_VARIANT(b64_p3q5_n45_pb8_h, double, 45, 3, 3, 5, false, 96, 1, 8, true)
+RBFB_BLK16_VARIANT(bmx_p3q5_n45_pb8_h, float, 45, 3, 3, 5, true, 96, 1, 8, true)

@@ -34,14 +34,15 @@ Variant make_variant(const char* name) {
 }
 
 template <typename T, int NMAX, int NRHS, int P, int Q, bool MIXED, int BLOCK, int MINB, int PB,
-          bool PF>
+          bool PF, int GW = 32>
 Variant make_blk_variant(const char* name) {
-    using C = BlkCfg<T, NMAX, NRHS, P, Q, MIXED, PB>;
+    using C = BlkCfg<T, NMAX, NRHS, P, Q, MIXED, PB, GW>;
     Variant v{};
     v.name = name;
-    v.kernel = reinterpret_cast<const void*>(&blk_kernel<T, NMAX, NRHS, P, Q, MIXED, BLOCK, MINB, PB, PF>);
+    v.kernel = reinterpret_cast<const void*>(
+        &blk_kernel<T, NMAX, NRHS, P, Q, MIXED, BLOCK, MINB, PB, PF, GW>);
     v.launch = [](dim3 grid, int block, size_t smem, cudaStream_t st, const AsmParams& p) {
-        blk_kernel<T, NMAX, NRHS, P, Q, MIXED, BLOCK, MINB, PB, PF><<<grid, block, smem, st>>>(p);
+        blk_kernel<T, NMAX, NRHS, P, Q, MIXED, BLOCK, MINB, PB, PF, GW><<<grid, block, smem, st>>>(p);
     };
     v.mixed = MIXED;
     v.P = P;
@@ -61,6 +62,14 @@ Variant make_blk_variant(const char* name) {
     namespace rbfb {                                                                           \
     Variant variant_##name() {                                                                 \
         return make_blk_variant<T, NMAX, NRHS, P, Q, MIXED, BLOCK, MINB, PB, PF>(#name);       \
+    }                                                                                          \
+    }
+
+// the same with half-warp groups: two stencils per warp
+#define RBFB_DEFINE_BLK16_VARIANT(name, T, NMAX, NRHS, P, Q, MIXED, BLOCK, MINB, PB, PF)        \
+    namespace rbfb {                                                                           \
+    Variant variant_##name() {                                                                 \
+        return make_blk_variant<T, NMAX, NRHS, P, Q, MIXED, BLOCK, MINB, PB, PF, 16>(#name);   \
     }                                                                                          \
     }
 

@@ -40,7 +40,7 @@ def nvcc() -> str:
 def _variant_lines():
     """(macro suffix, arguments) of every shape line of asm_variant_list.h."""
     text = (CSRC / "asm_variant_list.h").read_text()
-    return re.findall(r"^RBFB_(VARIANT|BLK_VARIANT)\((.*)\)\s*$", text, flags=re.M)
+    return re.findall(r"^RBFB_(VARIANT|BLK_VARIANT|BLK16_VARIANT)\((.*)\)\s*$", text, flags=re.M)
 
 
 def _sources():
