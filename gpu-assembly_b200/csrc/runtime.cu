@@ -120,7 +120,8 @@ int launch_variant(rbfb_ctx* ctx, int v, const AsmParams& p, cudaStream_t st, in
     }
     var.launch(dim3(grid), var.block, var.smem_block, st, p);
     ctx->launches.fetch_add(1, std::memory_order_relaxed);
-    RBFB_CUDA(ctx, cudaGetLastError());
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(ctx, e, (std::string("launch of ") + var.name).c_str());
     return RBFB_OK;
 }
 

@@ -240,6 +240,8 @@ def ref_lbm_lib():
         L.ref_lbm_bgk_split.argtypes = [C.c_int, C.c_int, C.c_double] + [C.c_void_p] * 5
         for nm in ("ref_lbm_feq", "ref_lbm_macros", "ref_lbm_bgk_split"):
             getattr(L, nm).restype = C.c_int
+        L.ref_lbm_error.argtypes = []
+        L.ref_lbm_error.restype = C.c_char_p
         _ref_lbm = L
     return _ref_lbm
 

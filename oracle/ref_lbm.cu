@@ -9,20 +9,26 @@
 // sum is rounded as the source writes it. Only the GPU tests load it: it pins
 // the library's LBM kernels to the reference's own, bit for bit. The
 // launchers take device pointers, check the launch and synchronise; they
-// allocate nothing. They return 0, or -1 (launch error) / -2 (run error).
+// allocate nothing. They return 0, or -1 (launch error) / -2 (run error),
+// and ref_lbm_error() names the CUDA error of the last failure.
 #include <cuda_runtime.h>
 
 #include "d2q9_kernels.cu"
 
 namespace {
+cudaError_t last_err = cudaSuccess;
 inline int grid(int n) { return (n + 255) / 256; }
 inline int done() {
-    if (cudaGetLastError() != cudaSuccess) return -1;
-    return cudaDeviceSynchronize() == cudaSuccess ? 0 : -2;
+    last_err = cudaGetLastError();
+    if (last_err != cudaSuccess) return -1;
+    last_err = cudaDeviceSynchronize();
+    return last_err == cudaSuccess ? 0 : -2;
 }
 }  // namespace
 
 extern "C" {
+
+const char* ref_lbm_error() { return cudaGetErrorString(last_err); }
 
 // precision 0: double arrays, 1: float arrays
 int ref_lbm_feq(int n, int precision, const void* rho, const void* ux, const void* uy, void* pdf) {

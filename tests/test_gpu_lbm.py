@@ -3,7 +3,8 @@
 * feq / macros / BGK (src/lbm/d2q9_kernels.cu:13-150), float and double:
   bit-identical to the oracle's CPU restatement and, where the reference's
   own kernels were built here (oracle/_ref/libref_lbm.so, compiled without
-  contraction), to the reference's kernels run on the same device arrays.
+  contraction), to the reference's kernels run on the same inputs in a
+  child process.
 * the fused streaming + collision step through interpolation operators
   assembled by this library at the 8 departure points x_s - c_a dt: bit-
   identical to the oracle's restatement of its summation order; a uniform
@@ -62,26 +63,74 @@ def test_collision_kernels_match_oracle_and_reference(torch_cuda, dtype):
     R.lbm_bgk(1.7, pdf, r2, u2, v2)  # bgk_kernel: no indp
     T.cuda.synchronize()
     np.testing.assert_array_equal(pdf.cpu().numpy(), post)
-    # the reference's own kernels on the same device arrays
-    L = O.ref_lbm_lib()
-    if L is None:
+    # the reference's own kernels, in a child process (the reference
+    # library carries its own CUDA runtime; it never loads in this one)
+    ref = _reference_kernels(dtype, rho, ux, uy, pert, 1.7)
+    if ref is None:
         return
-    prec = 0 if dtype == np.float64 else 1
-    ref = T.empty_like(pdf)
-    assert L.ref_lbm_feq(n, prec, rd.data_ptr(), ud.data_ptr(), vd.data_ptr(), ref.data_ptr()) == 0
-    np.testing.assert_array_equal(ref.cpu().numpy(), feq)
-    ref.copy_(_dev(T, pert))
-    r3, u3, v3, i3 = (T.empty_like(rd) for _ in range(4))
-    assert L.ref_lbm_bgk_split(n, prec, 1.7, ref.data_ptr(), r3.data_ptr(), u3.data_ptr(),
-                               v3.data_ptr(), i3.data_ptr()) == 0
-    np.testing.assert_array_equal(ref.cpu().numpy(), post)
-    for got, want in zip((r3, u3, v3, i3), (ro, uo, vo, io)):
-        np.testing.assert_array_equal(got.cpu().numpy(), want)
-    assert L.ref_lbm_macros(n, prec, ref.data_ptr(), r3.data_ptr(), u3.data_ptr(),
-                            v3.data_ptr()) == 0
-    mo = O.lbm_macros(post)
-    for got, want in zip((r3, u3, v3), mo):
-        np.testing.assert_array_equal(got.cpu().numpy(), want)
+    np.testing.assert_array_equal(ref["feq"], feq)
+    np.testing.assert_array_equal(ref["post"], post)
+    for nm, want in zip(("rho", "ux", "uy", "indp"), (ro, uo, vo, io)):
+        np.testing.assert_array_equal(ref[nm], want)
+    for nm, want in zip(("rho2", "ux2", "uy2"), O.lbm_macros(post)):
+        np.testing.assert_array_equal(ref[nm], want)
+
+
+CHILD = r"""
+import os
+import sys
+os.environ["CUDA_MODULE_LOADING"] = "EAGER"  # every module loaded when the runtime starts
+import numpy as np
+import torch as T
+sys.path.insert(0, sys.argv[2])
+import oracle as O
+d = sys.argv[1]
+L = O.ref_lbm_lib()
+a = {nm: T.as_tensor(np.load(f"{d}/{nm}.npy")).cuda() for nm in ("rho", "ux", "uy", "pert")}
+omega = float(np.load(f"{d}/omega.npy"))
+n = a["rho"].numel()
+prec = 0 if a["rho"].dtype == T.float64 else 1
+out = {}
+def ok(rc, what):
+    if rc != 0:
+        raise SystemExit(f"{what}: {rc} {L.ref_lbm_error().decode()}")
+pdf = T.empty(9 * n, dtype=a["rho"].dtype, device="cuda")
+ok(L.ref_lbm_feq(n, prec, a["rho"].data_ptr(), a["ux"].data_ptr(), a["uy"].data_ptr(),
+                 pdf.data_ptr()), "feq_kernel")
+out["feq"] = pdf.cpu().numpy()
+pdf.copy_(a["pert"])
+r, u, v, i = (T.empty_like(a["rho"]) for _ in range(4))
+ok(L.ref_lbm_bgk_split(n, prec, omega, pdf.data_ptr(), r.data_ptr(), u.data_ptr(), v.data_ptr(),
+                       i.data_ptr()), "bgk_kernel_split")
+out.update(post=pdf.cpu().numpy(), rho=r.cpu().numpy(), ux=u.cpu().numpy(),
+           uy=v.cpu().numpy(), indp=i.cpu().numpy())
+ok(L.ref_lbm_macros(n, prec, pdf.data_ptr(), r.data_ptr(), u.data_ptr(), v.data_ptr()),
+   "macros_kernel")
+out.update(rho2=r.cpu().numpy(), ux2=u.cpu().numpy(), uy2=v.cpu().numpy())
+np.savez(f"{d}/out.npz", **out)
+print("ok")
+"""
+
+
+def _reference_kernels(dtype, rho, ux, uy, pert, omega):
+    """The reference's feq / bgk_kernel_split / macros kernels run on the
+    given state in a child process: their outputs, or None when the
+    reference library was not built here."""
+    import subprocess
+    import sys
+    import tempfile
+    from pathlib import Path
+    if not O.REF_LBM_SO.exists():
+        return None
+    with tempfile.TemporaryDirectory() as d:
+        for nm, a in (("rho", rho), ("ux", ux), ("uy", uy), ("pert", pert)):
+            np.save(f"{d}/{nm}.npy", np.ascontiguousarray(a, dtype=dtype))
+        np.save(f"{d}/omega.npy", np.float64(omega))
+        r = subprocess.run([sys.executable, "-c", CHILD, d, str(Path(O.__file__).parent)],
+                           capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr[-3000:]
+        with np.load(f"{d}/out.npz") as z:
+            return {k: z[k] for k in z.files}
 
 
 def _streaming_operators(T, ctx, m=48, k=21, seed=3):

@@ -114,6 +114,22 @@ def test_range_and_shards_equal_the_whole(ctx, torch_cuda):
     full = [T.empty(n * k, dtype=T.float64, device="cuda") for _ in range(3)]
     ja = T.as_tensor(g["ja_nanoflann"]).cuda()
     ctx.assemble(d, x, y, k, ja, full)
+    T.cuda.synchronize()
+    # each range into outputs that start as NaN: every row written, every
+    # stencil's info set
+    for first, count in ((0, 1587), (1587, 1587), (3174, n - 3174)):
+        jr = ja[first * k:(first + count) * k].contiguous()
+        vr = [T.full((count * k,), float("nan"), dtype=T.float64, device="cuda")
+              for _ in range(3)]
+        ir = T.full((count,), -7, dtype=T.int32, device="cuda")
+        st = ctx.assemble_range(d, first, count, x, y, k, jr, vr, ir, stats=True)
+        T.cuda.synchronize()
+        assert st["stencils"] == count and (ir.cpu().numpy() == 0).all(), (first, st)
+        for q in range(3):
+            got = vr[q].cpu().numpy()
+            want = full[q][first * k:(first + count) * k].cpu().numpy()
+            bad = np.flatnonzero(got != want)
+            assert bad.size == 0, (first, q, bad.size, bad[:5] // k, got[bad[:3]], want[bad[:3]])
     parts_ja, parts_w = [], [[], [], []]
     for rank in range(3):  # three "ranks" on one GPU, one after another
         first, count, jr, vr = shard.assemble_shard(ctx, d, x, y, k, rank, 3)
@@ -123,7 +139,13 @@ def test_range_and_shards_equal_the_whole(ctx, torch_cuda):
     T.cuda.synchronize()
     np.testing.assert_array_equal(T.cat(parts_ja).cpu().numpy(), g["ja_nanoflann"])
     for q in range(3):
-        np.testing.assert_array_equal(T.cat(parts_w[q]).cpu().numpy(), full[q].cpu().numpy())
+        want = full[q].cpu().numpy()
+        at = 0
+        for rank in range(3):
+            got = parts_w[q][rank].cpu().numpy()
+            bad = np.flatnonzero(got != want[at:at + got.size])
+            assert bad.size == 0, (rank, q, bad.size, bad[:5] // k)
+            at += got.size
 
 
 def test_spmv_with_boundary_fix(ctx, torch_cuda):
