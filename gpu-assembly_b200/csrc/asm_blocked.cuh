@@ -290,9 +290,10 @@ __device__ __forceinline__ int eliminate_blocked(T* S, T* pinv, int* piv, int* a
             for (int v4 = 0; v4 < PB; v4 += VE) ldv(src + v4, &a[sl][v4]);
         }
         const int tend = min(PB, n - c0);  // steps in this panel
-        // look-ahead operands of the pivot search of the panel's first column
+        // look-ahead operands of the pivot search of the panel's first column:
+        // this lane's best key and its candidate value
         uint32_t pkey;
-        T pinvl;
+        T pbv;
         auto keys = [&](int t) {
             uint32_t best = 0;
             T bv = T(1);
@@ -305,7 +306,7 @@ __device__ __forceinline__ int eliminate_blocked(T* S, T* pinv, int* piv, int* a
                 }
             }
             pkey = best;
-            pinvl = recip_rn(bv);  // the oracle's 1 / pivot, if this lane owns the pivot
+            pbv = bv;
         };
         keys(0);
         // 2. the panel's steps
@@ -314,6 +315,9 @@ __device__ __forceinline__ int eliminate_blocked(T* S, T* pinv, int* piv, int* a
             if (t < tend) {
                 const int c = c0 + t;
                 const uint32_t mk = __reduce_max_sync(FULL, pkey);
+                // the oracle's 1 / pivot, if this lane owns the pivot: formed
+                // while the reduction is in flight
+                const T pinvl = recip_rn(pbv);
                 if (mk < 256u && info == 0) info = c + 1;  // zero pivot column
                 const int pos = 127 - (int)(mk & 127u);
                 const int owner = pos & (G - 1), osl = pos / G;
@@ -396,7 +400,8 @@ __device__ __forceinline__ int eliminate_blocked(T* S, T* pinv, int* piv, int* a
             bool any[R];
 #pragma unroll
             for (int sl = 0; sl < R; ++sl) any[sl] = __any_sync(FULL, kmask[sl] != 0u);
-#pragma unroll 1
+            // two column vectors per iteration: independent FMA chains
+#pragma unroll 2
             for (int v = 0; v < nv; ++v) {
                 const int col = jt + v * VE;
                 T u[PB][VE];
@@ -443,11 +448,27 @@ __device__ __forceinline__ void back_substitute_blk(const T* S, const T* pinv, c
     // Steps in segments of G from the last: in segment OS the owner of step c
     // holds it in slot OS (static), the slots below OS hold steps all before
     // c (updated unconditionally), the slots above OS steps all after it.
+    // The column of S and the reciprocal of step c - 1 are loaded during
+    // step c, so only the multiply -> shuffle -> fma chain is serial.
     auto segment = [&](auto os_c) {
         constexpr int OS = decltype(os_c)::value;
+        const int ctop = min(n, G * (OS + 1)) - 1;
+        if (ctop < G * OS) return;
+        T dvn = pinv[ctop];
+        T un[OS + 1];
+#pragma unroll
+        for (int sl = 0; sl <= OS; ++sl) un[sl] = S[prow_t[sl] * LDS + ctop];
 #pragma unroll 1
-        for (int c = min(n, G * (OS + 1)) - 1; c >= G * OS; --c) {
-            const T dv = pinv[c];
+        for (int c = ctop; c >= G * OS; --c) {
+            const T dv = dvn;
+            T uc[OS + 1];
+#pragma unroll
+            for (int sl = 0; sl <= OS; ++sl) uc[sl] = un[sl];
+            if (c > G * OS) {
+                dvn = pinv[c - 1];
+#pragma unroll
+                for (int sl = 0; sl <= OS; ++sl) un[sl] = S[prow_t[sl] * LDS + c - 1];
+            }
             T xq[NRHS];
 #pragma unroll
             for (int q = 0; q < NRHS; ++q) xq[q] = __shfl_sync(FULL, y[OS][q] * dv, c - G * OS, G);
@@ -457,8 +478,7 @@ __device__ __forceinline__ void back_substitute_blk(const T* S, const T* pinv, c
             }
 #pragma unroll
             for (int sl = 0; sl <= OS; ++sl) {
-                T u = S[prow_t[sl] * LDS + c];
-                if (sl == OS) u = (lane + G * sl < c) ? u : T(0);
+                const T u = (sl == OS && lane + G * sl >= c) ? T(0) : uc[sl];
 #pragma unroll
                 for (int q = 0; q < NRHS; ++q) y[sl][q] = fma(-u, xq[q], y[sl][q]);
             }

@@ -24,14 +24,12 @@ HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "_build" / "liboracle.so"
 REF_SO = HERE / "_ref" / "libref_knn.so"
 REF_FILL_SO = HERE / "_ref" / "libref_fill.so"
-REF_LBM_SO = HERE / "_ref" / "libref_lbm.so"
 
 OP_INTERP, OP_LAPLACE, OP_DX, OP_DY, OP_DXX, OP_DYY, OP_DXY = 1, 2, 4, 8, 16, 32, 64
 
 _lib = None
 _ref = None
 _ref_fill = None
-_ref_lbm = None
 
 _dp = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
 _ip = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
@@ -225,25 +223,6 @@ def lbm_stream_collide(k, ja, W, omega, pdf):
                                  pdf.ctypes.data, out.ctypes.data, rho.ctypes.data,
                                  ux.ctypes.data, uy.ctypes.data)
     return out, rho, ux, uy
-
-
-def ref_lbm_lib():
-    """The reference's own D2Q9 kernels (GPU; launchers take device
-    pointers), or None when not built here."""
-    global _ref_lbm
-    if _ref_lbm is None:
-        if not REF_LBM_SO.exists():
-            return None
-        L = C.CDLL(str(REF_LBM_SO))
-        L.ref_lbm_feq.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 4
-        L.ref_lbm_macros.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 4
-        L.ref_lbm_bgk_split.argtypes = [C.c_int, C.c_int, C.c_double] + [C.c_void_p] * 5
-        for nm in ("ref_lbm_feq", "ref_lbm_macros", "ref_lbm_bgk_split"):
-            getattr(L, nm).restype = C.c_int
-        L.ref_lbm_error.argtypes = []
-        L.ref_lbm_error.restype = C.c_char_p
-        _ref_lbm = L
-    return _ref_lbm
 
 
 def set_threads(n: int) -> None:

@@ -2,15 +2,15 @@
 // (feq_kernel, macros_kernel, bgk_kernel_split: src/lbm/d2q9_kernels.cu and
 // its header), for both instantiations.
 //
-// TEST INFRASTRUCTURE. oracle/Makefile compiles this file, which includes the
+// TEST INFRASTRUCTURE. ref_lbm_run.cu includes this file, which includes the
 // reference's d2q9_kernels.cu where it lies (nothing of it is copied here;
-// one translation unit, so the kernel templates and their launches meet),
-// into oracle/_ref/libref_lbm.so with --fmad=false, so that every product and
-// sum is rounded as the source writes it. Only the GPU tests load it: it pins
-// the library's LBM kernels to the reference's own, bit for bit. The
-// launchers take device pointers, check the launch and synchronise; they
-// allocate nothing. They return 0, or -1 (launch error) / -2 (run error),
-// and ref_lbm_error() names the CUDA error of the last failure.
+// one translation unit, so the kernel templates and their launches meet);
+// oracle/Makefile compiles that into oracle/_ref/ref_lbm_run with
+// --fmad=false, so that every product and sum is rounded as the source
+// writes it. It pins the library's LBM kernels to the reference's own, bit
+// for bit. The launchers take device pointers, check the launch and
+// synchronise; they allocate nothing. They return 0, or -1 (launch error) /
+// -2 (run error), and ref_lbm_error() names the CUDA error of the last failure.
 #include <cuda_runtime.h>
 
 #include "d2q9_kernels.cu"

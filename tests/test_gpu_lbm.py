@@ -2,14 +2,16 @@
 
 * feq / macros / BGK (src/lbm/d2q9_kernels.cu:13-150), float and double:
   bit-identical to the oracle's CPU restatement and, where the reference's
-  own kernels were built here (oracle/_ref/libref_lbm.so, compiled without
-  contraction), to the reference's kernels run on the same inputs in a
-  child process.
+  own kernels were built here (oracle/_ref/ref_lbm_run, compiled without
+  contraction), to the reference's kernels run on the same inputs by that
+  program, a process of its own.
 * the fused streaming + collision step through interpolation operators
   assembled by this library at the 8 departure points x_s - c_a dt: bit-
   identical to the oracle's restatement of its summation order; a uniform
   flow stays uniform.
 """
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -63,8 +65,8 @@ def test_collision_kernels_match_oracle_and_reference(torch_cuda, dtype):
     R.lbm_bgk(1.7, pdf, r2, u2, v2)  # bgk_kernel: no indp
     T.cuda.synchronize()
     np.testing.assert_array_equal(pdf.cpu().numpy(), post)
-    # the reference's own kernels, in a child process (the reference
-    # library carries its own CUDA runtime; it never loads in this one)
+    # the reference's own kernels, run by a program of their own (nothing of
+    # the reference loads into this process)
     ref = _reference_kernels(dtype, rho, ux, uy, pert, 1.7)
     if ref is None:
         return
@@ -76,61 +78,27 @@ def test_collision_kernels_match_oracle_and_reference(torch_cuda, dtype):
         np.testing.assert_array_equal(ref[nm], want)
 
 
-CHILD = r"""
-import os
-import sys
-os.environ["CUDA_MODULE_LOADING"] = "EAGER"  # every module loaded when the runtime starts
-import numpy as np
-import torch as T
-sys.path.insert(0, sys.argv[2])
-import oracle as O
-d = sys.argv[1]
-L = O.ref_lbm_lib()
-a = {nm: T.as_tensor(np.load(f"{d}/{nm}.npy")).cuda() for nm in ("rho", "ux", "uy", "pert")}
-omega = float(np.load(f"{d}/omega.npy"))
-n = a["rho"].numel()
-prec = 0 if a["rho"].dtype == T.float64 else 1
-out = {}
-def ok(rc, what):
-    if rc != 0:
-        raise SystemExit(f"{what}: {rc} {L.ref_lbm_error().decode()}")
-pdf = T.empty(9 * n, dtype=a["rho"].dtype, device="cuda")
-ok(L.ref_lbm_feq(n, prec, a["rho"].data_ptr(), a["ux"].data_ptr(), a["uy"].data_ptr(),
-                 pdf.data_ptr()), "feq_kernel")
-out["feq"] = pdf.cpu().numpy()
-pdf.copy_(a["pert"])
-r, u, v, i = (T.empty_like(a["rho"]) for _ in range(4))
-ok(L.ref_lbm_bgk_split(n, prec, omega, pdf.data_ptr(), r.data_ptr(), u.data_ptr(), v.data_ptr(),
-                       i.data_ptr()), "bgk_kernel_split")
-out.update(post=pdf.cpu().numpy(), rho=r.cpu().numpy(), ux=u.cpu().numpy(),
-           uy=v.cpu().numpy(), indp=i.cpu().numpy())
-ok(L.ref_lbm_macros(n, prec, pdf.data_ptr(), r.data_ptr(), u.data_ptr(), v.data_ptr()),
-   "macros_kernel")
-out.update(rho2=r.cpu().numpy(), ux2=u.cpu().numpy(), uy2=v.cpu().numpy())
-np.savez(f"{d}/out.npz", **out)
-print("ok")
-"""
-
-
 def _reference_kernels(dtype, rho, ux, uy, pert, omega):
     """The reference's feq / bgk_kernel_split / macros kernels run on the
-    given state in a child process: their outputs, or None when the
-    reference library was not built here."""
+    given state by oracle/_ref/ref_lbm_run, a process of its own: their
+    outputs, or None when the runner was not built here."""
     import subprocess
-    import sys
     import tempfile
-    from pathlib import Path
-    if not O.REF_LBM_SO.exists():
+    exe = Path(O.__file__).parent / "_ref" / "ref_lbm_run"
+    if not exe.exists():
         return None
+    n = rho.size
     with tempfile.TemporaryDirectory() as d:
         for nm, a in (("rho", rho), ("ux", ux), ("uy", uy), ("pert", pert)):
-            np.save(f"{d}/{nm}.npy", np.ascontiguousarray(a, dtype=dtype))
-        np.save(f"{d}/omega.npy", np.float64(omega))
-        r = subprocess.run([sys.executable, "-c", CHILD, d, str(Path(O.__file__).parent)],
+            np.ascontiguousarray(a, dtype=dtype).tofile(f"{d}/{nm}.bin")
+        prec = 0 if dtype == np.float64 else 1
+        r = subprocess.run([str(exe), d, str(n), str(prec), repr(float(omega))],
                            capture_output=True, text=True, timeout=600)
         assert r.returncode == 0 and "ok" in r.stdout, r.stdout + r.stderr[-3000:]
-        with np.load(f"{d}/out.npz") as z:
-            return {k: z[k] for k in z.files}
+        out = {}
+        for nm in ("feq", "post", "rho", "ux", "uy", "indp", "rho2", "ux2", "uy2"):
+            out[nm] = np.fromfile(f"{d}/{nm}.bin", dtype=dtype)
+        return out
 
 
 def _streaming_operators(T, ctx, m=48, k=21, seed=3):

@@ -131,12 +131,30 @@ def test_range_and_shards_equal_the_whole(ctx, torch_cuda):
             bad = np.flatnonzero(got != want)
             assert bad.size == 0, (first, q, bad.size, bad[:5] // k, got[bad[:3]], want[bad[:3]])
     parts_ja, parts_w = [], [[], [], []]
+    ja_h = g["ja_nanoflann"]
+    full_h = [f.cpu().numpy() for f in full]
+
+    def check(rank, first, count, jr, vr, when):
+        a, b = first * k, (first + count) * k
+        bad_ja = np.flatnonzero(jr.cpu().numpy() != ja_h[a:b])
+        assert bad_ja.size == 0, (when, rank, "ja", bad_ja.size, bad_ja[:4] // k,
+                                  jr.cpu().numpy()[bad_ja[:4]])
+        for q in range(3):
+            bad = np.flatnonzero(vr[q].cpu().numpy() != full_h[q][a:b])
+            assert bad.size == 0, (when, rank, "w", q, bad.size, bad[:4] // k)
+
+    shards = []
     for rank in range(3):  # three "ranks" on one GPU, one after another
         first, count, jr, vr = shard.assemble_shard(ctx, d, x, y, k, rank, 3)
+        T.cuda.synchronize()
+        check(rank, first, count, jr, vr, "right after its call")
+        shards.append((rank, first, count, jr, vr))
         parts_ja.append(jr)
         for q in range(3):
             parts_w[q].append(vr[q])
     T.cuda.synchronize()
+    for sh in shards:
+        check(*sh, "after all calls")
     np.testing.assert_array_equal(T.cat(parts_ja).cpu().numpy(), g["ja_nanoflann"])
     for q in range(3):
         want = full[q].cpu().numpy()
