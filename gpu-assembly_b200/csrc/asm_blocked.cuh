@@ -55,7 +55,7 @@ namespace rbfb {
 
 // Layout of one stencil's working set for systems of up to NMAX unknowns
 // with up to KMAX neighbours (shared memory, or a global scratch region).
-template <typename T, int NMAX, int NRHS, int KMAX_, int PB, int G_ = 32>
+template <typename T, int NMAX, int NRHS, int KMAX_, int PB, int G_ = 32, bool XBUF = true>
 struct BlkLayout {
     static constexpr int G = G_;  // lanes per stencil: a warp, or half of one
     static constexpr int KMAX = KMAX_;
@@ -77,7 +77,9 @@ struct BlkLayout {
     static constexpr int off_cy = off_cx + al16(8 * KMAX);
     static constexpr int off_s = off_cy + al16(8 * KMAX);
     static constexpr int off_x = off_s + al16(NMAX * LDS * (int)sizeof(T));
-    static constexpr int off_pinv = off_x + al16(NMAX * NRHS * (int)sizeof(T));
+    // the solution X (the refined form's sweeps read it; the FP64 form keeps
+    // it in registers and has no X)
+    static constexpr int off_pinv = off_x + (XBUF ? al16(NMAX * NRHS * (int)sizeof(T)) : 0);
     static constexpr int off_piv = off_pinv + al16(NMAX * (int)sizeof(T));
     static constexpr int off_act = off_piv + al16(4 * NMAX);
     static constexpr int off_alive = off_act + al16(4 * NMAX);
@@ -90,8 +92,8 @@ struct BlkLayout {
 };
 
 template <typename T, int NMAX, int NRHS, int P, int Q, bool MIXED, int PB, int G_ = 32>
-struct BlkCfg : BlkLayout<T, NMAX, NRHS, NMAX - npoly(P), PB, G_> {
-    using L = BlkLayout<T, NMAX, NRHS, NMAX - npoly(P), PB, G_>;
+struct BlkCfg : BlkLayout<T, NMAX, NRHS, NMAX - npoly(P), PB, G_, MIXED> {
+    using L = BlkLayout<T, NMAX, NRHS, NMAX - npoly(P), PB, G_, MIXED>;
     static_assert(MIXED ? sizeof(T) == 4 : sizeof(T) == 8,
                   "FP64 factors for the plain form, FP32 factors for the refined one");
     static constexpr int NP = npoly(P);
@@ -431,12 +433,17 @@ __device__ __forceinline__ int eliminate_blocked(T* S, T* pinv, int* piv, int* a
 // transformed right-hand sides of the rows pivoted at steps l, l + G, ...;
 // for c = n-1 .. 0 the owner of step c forms x_c = y * (1 / pivot_c) and
 // broadcasts it by shuffle, and the rows pivoted before c update with
-// u(row, c). X[c*NRHS + q] receives x_c.
-template <typename T, int R, int LDS, int NRHS, int G = 32>
+// u(row, c). The owner keeps x_c: xs[sl][q] of lane l is component
+// l + G*sl. With TOX, X[c*NRHS + q] also receives x_c.
+template <typename T, int R, int LDS, int NRHS, int G = 32, bool TOX = true>
 __device__ __forceinline__ void back_substitute_blk(const T* S, const T* pinv, const int* piv,
-                                                    T* X, int n, int lane) {
+                                                    T* X, int n, int lane, T (&xs)[R][NRHS]) {
     const unsigned FULL = group_mask(G);
     T y[R][NRHS];
+#pragma unroll
+    for (int sl = 0; sl < R; ++sl)
+#pragma unroll
+        for (int q = 0; q < NRHS; ++q) xs[sl][q] = T(0);
     int prow_t[R];
 #pragma unroll
     for (int sl = 0; sl < R; ++sl) {
@@ -470,9 +477,14 @@ __device__ __forceinline__ void back_substitute_blk(const T* S, const T* pinv, c
                 for (int sl = 0; sl <= OS; ++sl) un[sl] = S[prow_t[sl] * LDS + c - 1];
             }
             T xq[NRHS];
+            const bool own = lane == c - G * OS;
 #pragma unroll
-            for (int q = 0; q < NRHS; ++q) xq[q] = __shfl_sync(FULL, y[OS][q] * dv, c - G * OS, G);
-            if (lane == 0) {
+            for (int q = 0; q < NRHS; ++q) {
+                const T v = y[OS][q] * dv;
+                xq[q] = __shfl_sync(FULL, v, c - G * OS, G);
+                if (own) xs[OS][q] = v;
+            }
+            if (TOX && lane == 0) {
 #pragma unroll
                 for (int q = 0; q < NRHS; ++q) X[c * NRHS + q] = xq[q];
             }
@@ -594,17 +606,25 @@ __device__ __forceinline__ void residual_blk(T* S, const double* phi, const doub
 }
 
 // Scatter of the k node weights (unknowns NP .. NP+ks-1), rescaled,
-// src/rbf_operators.h:368-375; NaN for a singular stencil; info.
-template <typename T, int NRHS, int G = 32>
-__device__ __forceinline__ void scatter_blk(const AsmParams& p, const T* X, int np, int ks, int off,
-                                            int e, int info, int s, int lane) {
+// src/rbf_operators.h:368-375; NaN for a singular stencil; info. The
+// solution comes from the lanes' registers (xs of back_substitute_blk):
+// lane l writes the weights of unknowns l + G*sl.
+template <typename T, int R, int NRHS, int G = 32>
+__device__ __forceinline__ void scatter_regs(const AsmParams& p, const T (&xs)[R][NRHS], int np,
+                                             int ks, int off, int e, int info, int s, int lane) {
     const bool bad = info != 0;
-    for (int q = 0; q < p.nrhs; ++q) {
-        double* dst = out_column(p, q) + off;
-        const int sh = -op_order(p.col_op[q]) * e;
-        for (int j = lane; j < ks; j += G) {
-            const double v = static_cast<double>(X[(np + j) * NRHS + q]);
-            dst[j] = bad ? __longlong_as_double(0x7ff8000000000000ll) : scalbn(v, sh);
+#pragma unroll
+    for (int q = 0; q < NRHS; ++q) {
+        if (q < p.nrhs) {
+            double* dst = out_column(p, q) + off;
+            const int sh = -op_order(p.col_op[q]) * e;
+#pragma unroll
+            for (int sl = 0; sl < R; ++sl) {
+                const int j = lane + G * sl - np;
+                if (j >= 0 && j < ks)
+                    dst[j] = bad ? __longlong_as_double(0x7ff8000000000000ll)
+                                 : scalbn(static_cast<double>(xs[sl][q]), sh);
+            }
         }
     }
     if (lane == 0 && p.info) p.info[s - p.row_base] = info;
@@ -619,7 +639,7 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
     double* cx = reinterpret_cast<double*>(smem + C::off_cx);
     double* cy = reinterpret_cast<double*>(smem + C::off_cy);
     T* S = reinterpret_cast<T*>(smem + C::off_s);
-    T* X = reinterpret_cast<T*>(smem + C::off_x);
+    T* X = MIXED ? reinterpret_cast<T*>(smem + C::off_x) : nullptr;
     T* pinv = reinterpret_cast<T*>(smem + C::off_pinv);
     int* piv = reinterpret_cast<int*>(smem + C::off_piv);
     int* act = reinterpret_cast<int*>(smem + C::off_act);
@@ -695,9 +715,10 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
             cp_async8(cy + j, p.y + nb);
         }
     }
-    back_substitute_blk<T, R, LDS, NRHS, G>(S, pinv, piv, X, n, lane);
+    T xs[R][NRHS];
+    back_substitute_blk<T, R, LDS, NRHS, G, MIXED>(S, pinv, piv, X, n, lane, xs);
     if constexpr (!MIXED) {
-        scatter_blk<T, NRHS, G>(p, X, NP, ks, off, e, info, s, lane);
+        scatter_regs<T, R, NRHS, G>(p, xs, NP, ks, off, e, info, s, lane);
     } else {
         // ---- FP64 iterative refinement with the FP32 factors
         for (int i = lane; i < n * NRHS; i += G) x64[i] = static_cast<double>(X[i]);
@@ -713,7 +734,7 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
             ++sweeps;
             residual_blk<T, LDS, NRHS, NP, G>(S, phi, pm, x64, b64, ks, lane);
             forward_substitute_blk<T, R, LDS, NRHS, G>(S, piv, n, lane);
-            back_substitute_blk<T, R, LDS, NRHS, G>(S, pinv, piv, X, n, lane);
+            back_substitute_blk<T, R, LDS, NRHS, G, true>(S, pinv, piv, X, n, lane, xs);
             // x += d; convergence on max|d| / max|x| per right-hand side
             float worst = 0.f;
             for (int q = 0; q < p.nrhs; ++q) {
@@ -841,7 +862,6 @@ __device__ __forceinline__ void assemble_any(const AsmParams& p, int s, int off,
     double* cx = reinterpret_cast<double*>(base + L::off_cx);
     double* cy = reinterpret_cast<double*>(base + L::off_cy);
     T* S = reinterpret_cast<T*>(base + L::off_s);
-    T* X = reinterpret_cast<T*>(base + L::off_x);
     T* pinv = reinterpret_cast<T*>(base + L::off_pinv);
     int* piv = reinterpret_cast<int*>(base + L::off_piv);
     int* act = reinterpret_cast<int*>(base + L::off_act);
@@ -856,14 +876,15 @@ __device__ __forceinline__ void assemble_any(const AsmParams& p, int s, int off,
     }
     __syncwarp(group_mask(G));
     const int info = eliminate_blocked<T, L::R, LDS, NRHS, PB>(S, pinv, piv, act, alive, n, lane);
-    back_substitute_blk<T, L::R, LDS, NRHS>(S, pinv, piv, X, n, lane);
-    scatter_blk<T, NRHS>(p, X, np, ks, off, e, info, s, lane);
+    T xs[L::R][NRHS];
+    back_substitute_blk<T, L::R, LDS, NRHS, G, false>(S, pinv, piv, nullptr, n, lane, xs);
+    scatter_regs<T, L::R, NRHS, G>(p, xs, np, ks, off, e, info, s, lane);
 }
 
 template <typename T, int NS, int NG, int NRHS, int PB>
 struct CsrCfg {
-    using SmemL = BlkLayout<T, NS, NRHS, NS, PB>;    // shared-memory slot
-    using GlobL = BlkLayout<T, NG, NRHS, NG, PB>;    // global scratch region
+    using SmemL = BlkLayout<T, NS, NRHS, NS, PB, 32, false>;  // shared-memory slot
+    using GlobL = BlkLayout<T, NG, NRHS, NG, PB, 32, false>;  // global scratch region
     static constexpr size_t gbytes = (static_cast<size_t>(GlobL::bytes) + 255) & ~size_t(255);
 };
 

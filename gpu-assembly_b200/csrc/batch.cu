@@ -33,7 +33,7 @@ namespace {
 
 // The single-launch FP64 kernel for uneven batches: systems of up to 48
 // unknowns in shared memory (three warps per CTA), up to 96 in global scratch.
-constexpr int kOneNS = 48, kOneNG = 96, kOneBlock = 96, kOnePB = 8;
+constexpr int kOneNS = 48, kOneNG = 96, kOneBlock = 32, kOnePB = 8;
 using OneCfg = CsrCfg<double, kOneNS, kOneNG, 3, kOnePB>;
 constexpr int kOneSmem = OneCfg::SmemL::bytes * (kOneBlock / 32);
 
