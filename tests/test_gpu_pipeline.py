@@ -1,5 +1,7 @@
 """End-to-end host call, the uneven (CSR, bucketed) batch and the autotuner,
 each against the oracle or against the fixed-width device path."""
+import os
+
 import numpy as np
 import pytest
 
@@ -147,8 +149,22 @@ def test_range_and_shards_equal_the_whole(ctx, torch_cuda):
     for rank in range(3):  # three "ranks" on one GPU, one after another
         first, count, jr, vr = shard.assemble_shard(ctx, d, x, y, k, rank, 3)
         T.cuda.synchronize()
-        check(rank, first, count, jr, vr, "right after its call")
         shards.append((rank, first, count, jr, vr))
+        for sh in shards:
+            try:
+                check(*sh, f"after rank {rank}'s call")
+            except AssertionError:
+                diag = os.environ.get("RBFB_DIAG_DIR")
+                if diag:
+                    np.save(f"{diag}/shard{sh[0]}_ja_after{rank}.npy", sh[3].cpu().numpy())
+                    spans = [(r, "ja", t[3].data_ptr(), t[3].numel() * 4) for t in shards
+                             for r in [t[0]]]
+                    spans += [(t[0], f"w{q}", t[4][q].data_ptr(), t[4][q].numel() * 8)
+                              for t in shards for q in range(3)]
+                    with open(f"{diag}/spans_after{rank}.txt", "w") as f:
+                        for sp in spans:
+                            f.write(f"{sp[0]} {sp[1]} {sp[2]:#x} {sp[3]}\n")
+                raise
         parts_ja.append(jr)
         for q in range(3):
             parts_w[q].append(vr[q])
