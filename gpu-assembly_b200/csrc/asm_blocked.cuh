@@ -311,14 +311,16 @@ __device__ __forceinline__ int eliminate_blocked(T* S, T* pinv, int* piv, int* a
             pbv = bv;
         };
         keys(0);
+        // the reduction of step t is issued as soon as column t is updated
+        // (at the end of step t - 1), ahead of the rest of that update
+        uint32_t mk_next = __reduce_max_sync(FULL, pkey);
         // 2. the panel's steps
 #pragma unroll
         for (int t = 0; t < PB; ++t) {
             if (t < tend) {
                 const int c = c0 + t;
-                const uint32_t mk = __reduce_max_sync(FULL, pkey);
-                // the oracle's 1 / pivot, if this lane owns the pivot: formed
-                // while the reduction is in flight
+                const uint32_t mk = mk_next;
+                // the oracle's 1 / pivot, if this lane owns the pivot
                 const T pinvl = recip_rn(pbv);
                 if (mk < 256u && info == 0) info = c + 1;  // zero pivot column
                 const int pos = 127 - (int)(mk & 127u);
@@ -348,16 +350,22 @@ __device__ __forceinline__ int eliminate_blocked(T* S, T* pinv, int* piv, int* a
                     l[sl] = kmask[sl] ? a[sl][t] * inv : T(0);
                     a[sl][t] = l[sl];
                 }
-                // the panel columns right of c
+                // the panel columns right of c: column c + 1 first, then the
+                // next pivot search, then the rest
                 if (t + 1 < PB) {
                     T u[PB];
 #pragma unroll
                     for (int v4 = ((t + 1) / VE) * VE; v4 < PB; v4 += VE) ldv(U + v4, &u[v4]);
 #pragma unroll
-                    for (int j = t + 1; j < PB; ++j)
+                    for (int sl = 0; sl < R; ++sl) a[sl][t + 1] = fma(-l[sl], u[t + 1], a[sl][t + 1]);
+                    if (t + 1 < tend) {
+                        keys(t + 1);
+                        mk_next = __reduce_max_sync(FULL, pkey);
+                    }
+#pragma unroll
+                    for (int j = t + 2; j < PB; ++j)
 #pragma unroll
                         for (int sl = 0; sl < R; ++sl) a[sl][j] = fma(-l[sl], u[j], a[sl][j]);
-                    if (t + 1 < tend) keys(t + 1);
                 }
             }
         }
