@@ -146,28 +146,48 @@ def test_range_and_shards_equal_the_whole(ctx, torch_cuda):
             assert bad.size == 0, (when, rank, "w", q, bad.size, bad[:4] // k)
 
     shards = []
-    for rank in range(3):  # three "ranks" on one GPU, one after another
-        first, count, jr, vr = shard.assemble_shard(ctx, d, x, y, k, rank, 3)
-        T.cuda.synchronize()
-        shards.append((rank, first, count, jr, vr))
+    diag = os.environ.get("RBFB_DIAG_DIR")
+
+    def check_all(when):
         for sh in shards:
             try:
-                check(*sh, f"after rank {rank}'s call")
+                check(*sh, when)
             except AssertionError:
-                diag = os.environ.get("RBFB_DIAG_DIR")
                 if diag:
-                    np.save(f"{diag}/shard{sh[0]}_ja_after{rank}.npy", sh[3].cpu().numpy())
-                    spans = [(r, "ja", t[3].data_ptr(), t[3].numel() * 4) for t in shards
-                             for r in [t[0]]]
-                    spans += [(t[0], f"w{q}", t[4][q].data_ptr(), t[4][q].numel() * 8)
-                              for t in shards for q in range(3)]
-                    with open(f"{diag}/spans_after{rank}.txt", "w") as f:
-                        for sp in spans:
-                            f.write(f"{sp[0]} {sp[1]} {sp[2]:#x} {sp[3]}\n")
+                    np.save(f"{diag}/shard{sh[0]}_ja_{when.replace(' ', '_')}.npy",
+                            sh[3].cpu().numpy())
+                    with open(f"{diag}/spans.txt", "w") as f:
+                        for t in shards:
+                            f.write(f"{t[0]} ja {t[3].data_ptr():#x} {t[3].numel() * 4}\n")
+                            for q in range(3):
+                                f.write(f"{t[0]} w{q} {t[4][q].data_ptr():#x} "
+                                        f"{t[4][q].numel() * 8}\n")
                 raise
+
+    for rank in range(3):  # three "ranks" on one GPU, one after another
+        # shard.assemble_shard's steps, checked in between
+        first, count = shard.node_range(n, 3, rank)
+        jr = T.empty(count * k, dtype=T.int32, device="cuda")
+        vr = [T.empty(count * k, dtype=T.float64, device="cuda") for _ in range(3)]
+        ir = T.empty(count, dtype=T.int32, device="cuda")
+        xq, yq = x[first:first + count].contiguous(), y[first:first + count].contiguous()
+        ctx.knn_query(x, y, xq, yq, k, jr)
+        T.cuda.synchronize()
+        check_all(f"after rank {rank} knn")
+        bad = np.flatnonzero(jr.cpu().numpy() != ja_h[first * k:(first + count) * k])
+        assert bad.size == 0, ("own ja", rank, bad.size)
+        ctx.assemble_range(d, first, count, x, y, k, jr, vr, ir)
+        T.cuda.synchronize()
+        shards.append((rank, first, count, jr, vr))
+        check_all(f"after rank {rank} assembly")
         parts_ja.append(jr)
         for q in range(3):
             parts_w[q].append(vr[q])
+    # and the library's own helper
+    for rank in range(3):
+        first, count, jr, vr = shard.assemble_shard(ctx, d, x, y, k, rank, 3)
+        T.cuda.synchronize()
+        check(rank, first, count, jr, vr, "assemble_shard")
     T.cuda.synchronize()
     for sh in shards:
         check(*sh, "after all calls")
