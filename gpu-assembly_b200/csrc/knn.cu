@@ -670,7 +670,7 @@ int rbfb_knn_query(rbfb_ctx* ctx, int n, const double* x, const double* y, int n
     rc = knn::build(ctx, n, x, y, period_h, st);
     if (rc < 0) return rc;
     if (nq == 0) return RBFB_OK;
-    return knn::query(ctx, n, xq, yq, k, ja, st) == RBFB_OK
+    return knn::query(ctx, nq, xq, yq, k, ja, st) == RBFB_OK
                ? RBFB_OK
                : RBFB_ECUDA;
 }

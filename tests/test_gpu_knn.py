@@ -84,10 +84,14 @@ def test_query_points(ctx, torch_cuda):
     rng = np.random.default_rng(9)
     xq, yq = rng.uniform(-0.1, 1.1, 300), rng.uniform(-0.1, 1.1, 300)
     T = torch_cuda
-    ja = T.full((300 * 16,), -1, dtype=T.int32, device="cuda")
+    # 300 queries against 1600 nodes: the rows after the 300th (a guard region
+    # as long as the node set) stay untouched
+    buf = T.full((x.size * 16,), -1, dtype=T.int32, device="cuda")
+    ja = buf[: 300 * 16]
     ctx.knn_query(T.as_tensor(x).cuda(), T.as_tensor(y).cuda(), T.as_tensor(xq).cuda(),
                   T.as_tensor(yq).cuda(), 16, ja)
     np.testing.assert_array_equal(ja.cpu().numpy(), O.knn_brute(x, y, 16, xq=xq, yq=yq))
+    assert (buf[300 * 16:].cpu().numpy() == -1).all()
 
 
 def test_edge_cases(ctx, torch_cuda):

@@ -1,7 +1,5 @@
 """End-to-end host call, the uneven (CSR, bucketed) batch and the autotuner,
 each against the oracle or against the fixed-width device path."""
-import os
-
 import numpy as np
 import pytest
 
@@ -146,23 +144,10 @@ def test_range_and_shards_equal_the_whole(ctx, torch_cuda):
             assert bad.size == 0, (when, rank, "w", q, bad.size, bad[:4] // k)
 
     shards = []
-    diag = os.environ.get("RBFB_DIAG_DIR")
 
     def check_all(when):
         for sh in shards:
-            try:
-                check(*sh, when)
-            except AssertionError:
-                if diag:
-                    np.save(f"{diag}/shard{sh[0]}_ja_{when.replace(' ', '_')}.npy",
-                            sh[3].cpu().numpy())
-                    with open(f"{diag}/spans.txt", "w") as f:
-                        for t in shards:
-                            f.write(f"{t[0]} ja {t[3].data_ptr():#x} {t[3].numel() * 4}\n")
-                            for q in range(3):
-                                f.write(f"{t[0]} w{q} {t[4][q].data_ptr():#x} "
-                                        f"{t[4][q].numel() * 8}\n")
-                raise
+            check(*sh, when)
 
     for rank in range(3):  # three "ranks" on one GPU, one after another
         # shard.assemble_shard's steps, checked in between
@@ -188,9 +173,7 @@ def test_range_and_shards_equal_the_whole(ctx, torch_cuda):
         first, count, jr, vr = shard.assemble_shard(ctx, d, x, y, k, rank, 3)
         T.cuda.synchronize()
         check(rank, first, count, jr, vr, "assemble_shard")
-    T.cuda.synchronize()
-    for sh in shards:
-        check(*sh, "after all calls")
+    check_all("after all calls")
     np.testing.assert_array_equal(T.cat(parts_ja).cpu().numpy(), g["ja_nanoflann"])
     for q in range(3):
         want = full[q].cpu().numpy()
