@@ -17,6 +17,8 @@
 // system size n <= NMAX, panels of PB columns. RBFB_BLK16_VARIANT: the same
 // with half-warp groups, two stencils per warp.
 // The build compiles each line as its own translation unit.
+RBFB_VARIANT(f64_p4q7_n64_smem, double, 16, 2, 64, 3, 4, 7, false, 32, 1, true, true)
+RBFB_VARIANT(f64_p4q7_n80_smem, double, 16, 2, 80, 3, 4, 7, false, 32, 1, true, true)
 RBFB_BLK_VARIANT(b64_p3q5_n45_pb8, double, 45, 3, 3, 5, false, 32, 1, 8, true)
 RBFB_BLK_VARIANT(b64_p3q5_n45_pb8x3, double, 45, 3, 3, 5, false, 96, 1, 8, true)
 RBFB_BLK16_VARIANT(b64_p3q5_n45_pb8_h1, double, 45, 3, 3, 5, false, 32, 1, 8, true)
@@ -37,7 +39,5 @@ RBFB_VARIANT(mix_p2q3_n32_g16x1, float, 16, 1, 32, 3, 2, 3, true, 64, 1, false, 
 RBFB_VARIANT(mix_p2q3_n32_g16x2, float, 16, 2, 32, 3, 2, 3, true, 64, 1, false, true)
 RBFB_VARIANT(mix_p3q5_n48_g16x2, float, 16, 2, 48, 3, 3, 5, true, 64, 4, false, true)
 RBFB_VARIANT(mix_p3q5_n48_g16x1, float, 16, 1, 48, 3, 3, 5, true, 64, 1, false, true)
-RBFB_VARIANT(f64_p4q7_n64_smem, double, 16, 2, 64, 3, 4, 7, false, 32, 1, true, true)
-RBFB_VARIANT(f64_p4q7_n80_smem, double, 16, 2, 80, 3, 4, 7, false, 32, 1, true, true)
 RBFB_VARIANT(mix_p4q7_n64_smem, float, 16, 2, 64, 3, 4, 7, true, 32, 1, true, true)
 RBFB_VARIANT(mix_p4q7_n80_smem, float, 16, 2, 80, 3, 4, 7, true, 32, 1, true, true)
