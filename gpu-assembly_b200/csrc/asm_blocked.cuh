@@ -79,14 +79,22 @@ struct BlkLayout {
     static constexpr int off_x = off_s + al16(NMAX * LDS * (int)sizeof(T));
     // the solution X (the refined form's sweeps read it; the FP64 form keeps
     // it in registers and has no X)
-    static constexpr int off_pinv = off_x + (XBUF ? al16(NMAX * NRHS * (int)sizeof(T)) : 0);
-    static constexpr int off_piv = off_pinv + al16(NMAX * (int)sizeof(T));
-    static constexpr int off_act = off_piv + al16(4 * NMAX);
+    static constexpr int off_end = off_x + (XBUF ? al16(NMAX * NRHS * (int)sizeof(T)) : 0);
+    // The elimination's bookkeeping (the list of unused rows, their flags,
+    // the pivot order) and the next stencil's prefetched ja row. In the FP64
+    // form they share the neighbour-coordinate slots, which are idle from
+    // the end of the fill until the next stencil's coordinates are fetched
+    // (after the pivot order has been read by the back substitution); the
+    // refined form, whose sweeps read the pivot order again, keeps them apart.
+    static constexpr int BOOK = al16(4 * NMAX) + al16(NMAX) + al16(4 * NMAX) + al16(4 * KMAX);
+    static constexpr bool SHARE = !XBUF && BOOK <= off_s;
+    static constexpr int off_act = SHARE ? off_cx : off_end;
     static constexpr int off_alive = off_act + al16(4 * NMAX);
-    // next stencil, prefetched while this one is solved: its ja row, its
-    // centre (x, y) and its CSR bounds ia[s], ia[s + 1] (+ size, next item)
-    static constexpr int off_nja = off_alive + al16(NMAX);
-    static constexpr int off_nxy = off_nja + al16(4 * KMAX);
+    static constexpr int off_piv = off_alive + al16(NMAX);
+    static constexpr int off_nja = off_piv + al16(4 * NMAX);
+    // next stencil's centre (x, y) and CSR bounds ia[s], ia[s + 1] (+ size,
+    // next item)
+    static constexpr int off_nxy = SHARE ? off_end : off_nja + al16(4 * KMAX);
     static constexpr int off_nia = off_nxy + 16;
     static constexpr int bytes = off_nia + 16;
 };
@@ -136,7 +144,7 @@ __device__ __forceinline__ uint32_t hiword(double v) {
 __device__ __forceinline__ uint32_t hiword(float v) { return __float_as_uint(v); }
 
 // ---- the phases of one stencil, shared by the fixed-shape and the uneven
-// kernels. A stencil's working set (S, X, pinv, piv, act, alive, cx, cy) is
+// kernels. A stencil's working set (S, X, piv, act, alive, cx, cy) is
 // in shared memory, or -- for the uneven kernel's large stencils -- in a
 // global scratch region of the same layout.
 
@@ -188,14 +196,13 @@ __device__ __forceinline__ int gather_scale(const AsmParams& p, int off, int ks,
 // The augmented system in S (row stride LDS): phi block (each unordered pair
 // once, a flat walk over the lanes), monomial rows and columns, zero
 // polynomial block, right-hand sides as columns n .. n+NRHS-1 (fill_matrix /
-// fill_rhs, src/rbf_operators.h:116-185); alive[r] = r < n for r < nmax.
+// fill_rhs, src/rbf_operators.h:116-185).
 // With phi != nullptr (the refined form) the FP64 values are also kept: phi
 // (pair (i, j), i < j, at its number in row-major order of the strict upper
 // triangle), pm[i*NP + m] (monomials of node i) and b64[r*NRHS + q].
 template <typename T, int LDS, int NRHS, int P, int Q, int G = 32>
 __device__ __forceinline__ void fill_system(const AsmParams& p, T* S, const double* cx,
-                                            const double* cy, int ks, int e,
-                                            unsigned char* alive, int nmax, int lane,
+                                            const double* cy, int ks, int e, int lane,
                                             double* phi = nullptr, double* pm = nullptr,
                                             double* b64 = nullptr) {
     constexpr int NP = npoly(P);
@@ -250,20 +257,21 @@ __device__ __forceinline__ void fill_system(const AsmParams& p, T* S, const doub
             if (b64) b64[r * NRHS + q] = v;
         }
     }
-    for (int r = lane; r < nmax; r += G) alive[r] = r < n ? 1 : 0;
 }
 
 // Blocked right-looking elimination of the n x n system in S with its NRHS
 // right-hand-side columns (panels of PB; R list positions per lane, R*32 >=
 // n). Returns info: 0, or c + 1 for the first zero pivot.
 template <typename T, int R, int LDS, int NRHS, int PB, int G = 32>
-__device__ __forceinline__ int eliminate_blocked(T* S, T* pinv, int* piv, int* act,
-                                                 unsigned char* alive, int n, int lane) {
+__device__ __forceinline__ int eliminate_blocked(T* S, int* piv, int* act, unsigned char* alive,
+                                                 int n, int lane) {
     constexpr int VE = 16 / (int)sizeof(T);
     const unsigned FULL = group_mask(G);  // the group's lanes
     const int gbase = (threadIdx.x & 31) & ~(G - 1);
     const int W = n + NRHS;  // columns in use
     int info = 0;
+    for (int r = lane; r < n; r += G) alive[r] = 1;
+    __syncwarp(group_mask(G));
 #pragma unroll 1
     for (int c0 = 0; c0 < n; c0 += PB) {
         // 1. the unused rows, ascending, and this lane's panel rows
@@ -325,6 +333,7 @@ __device__ __forceinline__ int eliminate_blocked(T* S, T* pinv, int* piv, int* a
                 if (mk < 256u && info == 0) info = c + 1;  // zero pivot column
                 const int pos = 127 - (int)(mk & 127u);
                 const int owner = pos & (G - 1), osl = pos / G;
+                const T inv = __shfl_sync(FULL, pinvl, owner, G);
                 if (lane == owner) {
 #pragma unroll
                     for (int sl = 0; sl < R; ++sl) {
@@ -338,10 +347,8 @@ __device__ __forceinline__ int eliminate_blocked(T* S, T* pinv, int* piv, int* a
                             kcon[sl] = 0u;
                         }
                     }
-                    pinv[c] = pinvl;
                 }
                 __syncwarp(group_mask(G));
-                const T inv = pinv[c];
                 const T* U = S + piv[c] * LDS + c0;
                 // multipliers of the unused rows (0 for the others)
                 T l[R];
@@ -442,10 +449,20 @@ __device__ __forceinline__ int eliminate_blocked(T* S, T* pinv, int* piv, int* a
 // for c = n-1 .. 0 the owner of step c forms x_c = y * (1 / pivot_c) and
 // broadcasts it by shuffle, and the rows pivoted before c update with
 // u(row, c). The owner keeps x_c: xs[sl][q] of lane l is component
-// l + G*sl. With TOX, X[c*NRHS + q] also receives x_c.
-template <typename T, int R, int LDS, int NRHS, int G = 32, bool TOX = true>
-__device__ __forceinline__ void back_substitute_blk(const T* S, const T* pinv, const int* piv,
-                                                    T* X, int n, int lane, T (&xs)[R][NRHS]) {
+// l + G*sl. With TOX, X[c*NRHS + q] also receives x_c. Each lane forms
+// 1 / pivot of its own steps from the pivots in S (the same rounding as
+// the elimination's), and `after_loads` runs once the pivot order has been
+// read (it may reuse the bookkeeping slots). Steps below `cstop` are not
+// taken: x_c depends only on the x of later steps, so a caller that needs
+// the unknowns cstop .. n-1 alone (the weights, after the polynomial
+// multipliers) gets them unchanged.
+struct NoHook {
+    __device__ void operator()() const {}
+};
+template <typename T, int R, int LDS, int NRHS, int G = 32, bool TOX = true, class Hook = NoHook>
+__device__ __forceinline__ void back_substitute_blk(const T* S, const int* piv, T* X, int n,
+                                                    int lane, T (&xs)[R][NRHS],
+                                                    Hook after_loads = Hook{}, int cstop = 0) {
     const unsigned FULL = group_mask(G);
     T y[R][NRHS];
 #pragma unroll
@@ -453,34 +470,36 @@ __device__ __forceinline__ void back_substitute_blk(const T* S, const T* pinv, c
 #pragma unroll
         for (int q = 0; q < NRHS; ++q) xs[sl][q] = T(0);
     int prow_t[R];
+    T dvown[R];  // 1 / pivot of this lane's steps
 #pragma unroll
     for (int sl = 0; sl < R; ++sl) {
         const int t = lane + G * sl;
         prow_t[sl] = t < n ? piv[t] : 0;
 #pragma unroll
         for (int q = 0; q < NRHS; ++q) y[sl][q] = t < n ? S[prow_t[sl] * LDS + n + q] : T(0);
+        dvown[sl] = t < n ? recip_rn(S[prow_t[sl] * LDS + t]) : T(0);
     }
+    __syncwarp(group_mask(G));
+    after_loads();
     // Steps in segments of G from the last: in segment OS the owner of step c
     // holds it in slot OS (static), the slots below OS hold steps all before
     // c (updated unconditionally), the slots above OS steps all after it.
-    // The column of S and the reciprocal of step c - 1 are loaded during
-    // step c, so only the multiply -> shuffle -> fma chain is serial.
+    // The column of S of step c - 1 is loaded during step c, so only the
+    // multiply -> shuffle -> fma chain is serial.
     auto segment = [&](auto os_c) {
         constexpr int OS = decltype(os_c)::value;
         const int ctop = min(n, G * (OS + 1)) - 1;
-        if (ctop < G * OS) return;
-        T dvn = pinv[ctop];
+        const int cend = max(G * OS, cstop);  // last step of the segment
+        if (ctop < cend) return;
         T un[OS + 1];
 #pragma unroll
         for (int sl = 0; sl <= OS; ++sl) un[sl] = S[prow_t[sl] * LDS + ctop];
 #pragma unroll 1
-        for (int c = ctop; c >= G * OS; --c) {
-            const T dv = dvn;
+        for (int c = ctop; c >= cend; --c) {
             T uc[OS + 1];
 #pragma unroll
             for (int sl = 0; sl <= OS; ++sl) uc[sl] = un[sl];
-            if (c > G * OS) {
-                dvn = pinv[c - 1];
+            if (c > cend) {
 #pragma unroll
                 for (int sl = 0; sl <= OS; ++sl) un[sl] = S[prow_t[sl] * LDS + c - 1];
             }
@@ -488,7 +507,7 @@ __device__ __forceinline__ void back_substitute_blk(const T* S, const T* pinv, c
             const bool own = lane == c - G * OS;
 #pragma unroll
             for (int q = 0; q < NRHS; ++q) {
-                const T v = y[OS][q] * dv;
+                const T v = y[OS][q] * dvown[OS];  // the owner's value is x_c
                 xq[q] = __shfl_sync(FULL, v, c - G * OS, G);
                 if (own) xs[OS][q] = v;
             }
@@ -648,7 +667,6 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
     double* cy = reinterpret_cast<double*>(smem + C::off_cy);
     T* S = reinterpret_cast<T*>(smem + C::off_s);
     T* X = MIXED ? reinterpret_cast<T*>(smem + C::off_x) : nullptr;
-    T* pinv = reinterpret_cast<T*>(smem + C::off_pinv);
     int* piv = reinterpret_cast<int*>(smem + C::off_piv);
     int* act = reinterpret_cast<int*>(smem + C::off_act);
     unsigned char* alive = reinterpret_cast<unsigned char*>(smem + C::off_alive);
@@ -690,7 +708,10 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
         }
     }
     const int e = gather_scale<C::KMAX, PF, G>(p, off, ks, x0, y0, cx, cy, lane);
-    fill_system<T, LDS, NRHS, P, Q, G>(p, S, cx, cy, ks, e, alive, NMAX, lane, phi, pm, b64);
+    fill_system<T, LDS, NRHS, P, Q, G>(p, S, cx, cy, ks, e, lane, phi, pm, b64);
+    // the coordinate slots are read: with C::SHARE the bookkeeping and the
+    // next ja row may now take them
+    __syncwarp(group_mask(G));
 
     // prefetch stage 2: the next stencil's ja row (its bounds have landed)
     if constexpr (PF) {
@@ -712,19 +733,40 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
     }
     __syncwarp(group_mask(G));
 
-    const int info = eliminate_blocked<T, R, LDS, NRHS, PB, G>(S, pinv, piv, act, alive, n, lane);
+    const int info = eliminate_blocked<T, R, LDS, NRHS, PB, G>(S, piv, act, alive, n, lane);
 
-    // prefetch stage 3: the next stencil's neighbour coordinates into cx/cy
-    if (const int ksn = PF ? nia[2] : 0; ksn > 0) {
-        cp_async_wait_all();
-        for (int j = lane; j < ksn; j += G) {
-            const int nb = nja[j];
-            cp_async8(cx + j, p.x + nb);
-            cp_async8(cy + j, p.y + nb);
+    // prefetch stage 3: the next stencil's neighbour coordinates into cx/cy,
+    // once the back substitution has read the pivot order: every lane reads
+    // its ja slots first, then the copies may land on the shared slots
+    auto stage3 = [&]() {
+        if constexpr (PF) {
+            constexpr int KPL = (C::KMAX + G - 1) / G;
+            const int ksn = nia[2];
+            if (ksn > 0) {
+                cp_async_wait_all();
+                int nb[KPL];
+#pragma unroll
+                for (int t = 0; t < KPL; ++t) {
+                    const int j = lane + G * t;
+                    nb[t] = j < ksn ? nja[j] : 0;
+                }
+                __syncwarp(group_mask(G));
+#pragma unroll
+                for (int t = 0; t < KPL; ++t) {
+                    const int j = lane + G * t;
+                    if (j < ksn) {
+                        cp_async8(cx + j, p.x + nb[t]);
+                        cp_async8(cy + j, p.y + nb[t]);
+                    }
+                }
+            }
         }
-    }
+    };
     T xs[R][NRHS];
-    back_substitute_blk<T, R, LDS, NRHS, G, MIXED>(S, pinv, piv, X, n, lane, xs);
+    // the FP64 form needs the weights alone (unknowns NP .. n-1); the refined
+    // form's residual needs every unknown
+    back_substitute_blk<T, R, LDS, NRHS, G, MIXED>(S, piv, X, n, lane, xs, stage3,
+                                                   MIXED ? 0 : NP);
     if constexpr (!MIXED) {
         scatter_regs<T, R, NRHS, G>(p, xs, NP, ks, off, e, info, s, lane);
     } else {
@@ -742,7 +784,7 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
             ++sweeps;
             residual_blk<T, LDS, NRHS, NP, G>(S, phi, pm, x64, b64, ks, lane);
             forward_substitute_blk<T, R, LDS, NRHS, G>(S, piv, n, lane);
-            back_substitute_blk<T, R, LDS, NRHS, G, true>(S, pinv, piv, X, n, lane, xs);
+            back_substitute_blk<T, R, LDS, NRHS, G, true>(S, piv, X, n, lane, xs);
             // x += d; convergence on max|d| / max|x| per right-hand side
             float worst = 0.f;
             for (int q = 0; q < p.nrhs; ++q) {
@@ -798,6 +840,49 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
     }
 }
 
+// The prefetch of a group's first stencil, done up front: centre and CSR
+// bounds, then the ja row, then the neighbour coordinates into cx/cy (every
+// lane reads its ja slots before any copy may land on shared slots).
+template <class C>
+__device__ __forceinline__ void prefetch_first_blk(const AsmParams& p, int s, char* smem,
+                                                   int lane) {
+    constexpr int G = C::G, KPL = (C::KMAX + G - 1) / G;
+    double* cx = reinterpret_cast<double*>(smem + C::off_cx);
+    double* cy = reinterpret_cast<double*>(smem + C::off_cy);
+    int* nja = reinterpret_cast<int*>(smem + C::off_nja);
+    double* nxy = reinterpret_cast<double*>(smem + C::off_nxy);
+    int* nia = reinterpret_cast<int*>(smem + C::off_nia);
+    if (lane == 0) {
+        cp_async8(nxy, p.x + s);
+        cp_async8(nxy + 1, p.y + s);
+        if (p.ia) {
+            cp_async4(nia, p.ia + s);
+            cp_async4(nia + 1, p.ia + s + 1);
+        }
+    }
+    cp_async_wait_all();
+    __syncwarp(group_mask(G));
+    const int off = p.ia ? nia[0] : (s - p.row_base) * p.k;
+    const int ks = p.ia ? nia[1] - off : p.k;
+    for (int j = lane; j < ks; j += G) cp_async4(nja + j, p.ja + off + j);
+    cp_async_wait_all();
+    int nb[KPL];
+#pragma unroll
+    for (int t = 0; t < KPL; ++t) {
+        const int j = lane + G * t;
+        nb[t] = j < ks ? nja[j] : 0;
+    }
+    __syncwarp(group_mask(G));
+#pragma unroll
+    for (int t = 0; t < KPL; ++t) {
+        const int j = lane + G * t;
+        if (j < ks) {
+            cp_async8(cx + j, p.x + nb[t]);
+            cp_async8(cy + j, p.y + nb[t]);
+        }
+    }
+}
+
 template <typename T, int NMAX, int NRHS, int P, int Q, bool MIXED, int BLOCK, int MINB, int PB,
           bool PF, int GW = 32>
 __global__ void __launch_bounds__(BLOCK, MINB) blk_kernel(AsmParams p) {
@@ -824,7 +909,7 @@ __global__ void __launch_bounds__(BLOCK, MINB) blk_kernel(AsmParams p) {
     int* next_it = reinterpret_cast<int*>(smem + C::off_nia) + 3;
     int it = claim(blockIdx.x * GPB + gib);
     if constexpr (PF) {
-        if (it < n) prefetch_first<C>(p, item(it), smem, lane, gmask);
+        if (it < n) prefetch_first_blk<C>(p, item(it), smem, lane);
     }
     while (it < n) {
         const int itn = claim(it + ngroups);
@@ -851,13 +936,12 @@ __global__ void __launch_bounds__(BLOCK, MINB) blk_kernel(AsmParams p) {
 // Runtime-Q dispatch of the fill (the elimination does not depend on P or Q).
 template <typename T, int LDS, int NRHS, int P>
 __device__ __forceinline__ void fill_system_q(const AsmParams& p, int Q, T* S, const double* cx,
-                                              const double* cy, int ks, int e,
-                                              unsigned char* alive, int nmax, int lane) {
+                                              const double* cy, int ks, int e, int lane) {
     switch (Q) {
-        case 3: fill_system<T, LDS, NRHS, P, 3>(p, S, cx, cy, ks, e, alive, nmax, lane); break;
-        case 5: fill_system<T, LDS, NRHS, P, 5>(p, S, cx, cy, ks, e, alive, nmax, lane); break;
-        case 7: fill_system<T, LDS, NRHS, P, 7>(p, S, cx, cy, ks, e, alive, nmax, lane); break;
-        default: fill_system<T, LDS, NRHS, P, 9>(p, S, cx, cy, ks, e, alive, nmax, lane); break;
+        case 3: fill_system<T, LDS, NRHS, P, 3>(p, S, cx, cy, ks, e, lane); break;
+        case 5: fill_system<T, LDS, NRHS, P, 5>(p, S, cx, cy, ks, e, lane); break;
+        case 7: fill_system<T, LDS, NRHS, P, 7>(p, S, cx, cy, ks, e, lane); break;
+        default: fill_system<T, LDS, NRHS, P, 9>(p, S, cx, cy, ks, e, lane); break;
     }
 }
 
@@ -870,22 +954,21 @@ __device__ __forceinline__ void assemble_any(const AsmParams& p, int s, int off,
     double* cx = reinterpret_cast<double*>(base + L::off_cx);
     double* cy = reinterpret_cast<double*>(base + L::off_cy);
     T* S = reinterpret_cast<T*>(base + L::off_s);
-    T* pinv = reinterpret_cast<T*>(base + L::off_pinv);
     int* piv = reinterpret_cast<int*>(base + L::off_piv);
     int* act = reinterpret_cast<int*>(base + L::off_act);
     unsigned char* alive = reinterpret_cast<unsigned char*>(base + L::off_alive);
     const int np = npoly(P), n = np + ks;
     const int e = gather_scale<L::KMAX, false>(p, off, ks, p.x[s], p.y[s], cx, cy, lane);
     switch (P) {
-        case 1: fill_system_q<T, LDS, NRHS, 1>(p, Q, S, cx, cy, ks, e, alive, n, lane); break;
-        case 2: fill_system_q<T, LDS, NRHS, 2>(p, Q, S, cx, cy, ks, e, alive, n, lane); break;
-        case 3: fill_system_q<T, LDS, NRHS, 3>(p, Q, S, cx, cy, ks, e, alive, n, lane); break;
-        default: fill_system_q<T, LDS, NRHS, 4>(p, Q, S, cx, cy, ks, e, alive, n, lane); break;
+        case 1: fill_system_q<T, LDS, NRHS, 1>(p, Q, S, cx, cy, ks, e, lane); break;
+        case 2: fill_system_q<T, LDS, NRHS, 2>(p, Q, S, cx, cy, ks, e, lane); break;
+        case 3: fill_system_q<T, LDS, NRHS, 3>(p, Q, S, cx, cy, ks, e, lane); break;
+        default: fill_system_q<T, LDS, NRHS, 4>(p, Q, S, cx, cy, ks, e, lane); break;
     }
     __syncwarp(group_mask(G));
-    const int info = eliminate_blocked<T, L::R, LDS, NRHS, PB>(S, pinv, piv, act, alive, n, lane);
+    const int info = eliminate_blocked<T, L::R, LDS, NRHS, PB>(S, piv, act, alive, n, lane);
     T xs[L::R][NRHS];
-    back_substitute_blk<T, L::R, LDS, NRHS, G, false>(S, pinv, piv, nullptr, n, lane, xs);
+    back_substitute_blk<T, L::R, LDS, NRHS, G, false>(S, piv, nullptr, n, lane, xs, NoHook{}, np);
     scatter_regs<T, L::R, NRHS, G>(p, xs, np, ks, off, e, info, s, lane);
 }
 
