@@ -96,7 +96,11 @@ struct BlkLayout {
     // next item)
     static constexpr int off_nxy = SHARE ? off_end : off_nja + al16(4 * KMAX);
     static constexpr int off_nia = off_nxy + 16;
-    static constexpr int bytes = off_nia + 16;
+    // 1 / pivot of every step, written by the step's owner and read by all
+    // lanes (a shared-memory broadcast measured faster than a shuffle in the
+    // uneven kernel) and by the back substitution
+    static constexpr int off_pinv = off_nia + 16;
+    static constexpr int bytes = off_pinv + al16(NMAX * (int)sizeof(T));
 };
 
 template <typename T, int NMAX, int NRHS, int P, int Q, bool MIXED, int PB, int G_ = 32>
@@ -144,7 +148,7 @@ __device__ __forceinline__ uint32_t hiword(double v) {
 __device__ __forceinline__ uint32_t hiword(float v) { return __float_as_uint(v); }
 
 // ---- the phases of one stencil, shared by the fixed-shape and the uneven
-// kernels. A stencil's working set (S, X, piv, act, alive, cx, cy) is
+// kernels. A stencil's working set (S, X, pinv, piv, act, alive, cx, cy) is
 // in shared memory, or -- for the uneven kernel's large stencils -- in a
 // global scratch region of the same layout.
 
@@ -263,8 +267,8 @@ __device__ __forceinline__ void fill_system(const AsmParams& p, T* S, const doub
 // right-hand-side columns (panels of PB; R list positions per lane, R*32 >=
 // n). Returns info: 0, or c + 1 for the first zero pivot.
 template <typename T, int R, int LDS, int NRHS, int PB, int G = 32>
-__device__ __forceinline__ int eliminate_blocked(T* S, int* piv, int* act, unsigned char* alive,
-                                                 int n, int lane) {
+__device__ __forceinline__ int eliminate_blocked(T* S, T* pinv, int* piv, int* act,
+                                                 unsigned char* alive, int n, int lane) {
     constexpr int VE = 16 / (int)sizeof(T);
     const unsigned FULL = group_mask(G);  // the group's lanes
     const int gbase = (threadIdx.x & 31) & ~(G - 1);
@@ -333,7 +337,6 @@ __device__ __forceinline__ int eliminate_blocked(T* S, int* piv, int* act, unsig
                 if (mk < 256u && info == 0) info = c + 1;  // zero pivot column
                 const int pos = 127 - (int)(mk & 127u);
                 const int owner = pos & (G - 1), osl = pos / G;
-                const T inv = __shfl_sync(FULL, pinvl, owner, G);
                 if (lane == owner) {
 #pragma unroll
                     for (int sl = 0; sl < R; ++sl) {
@@ -347,8 +350,10 @@ __device__ __forceinline__ int eliminate_blocked(T* S, int* piv, int* act, unsig
                             kcon[sl] = 0u;
                         }
                     }
+                    pinv[c] = pinvl;
                 }
                 __syncwarp(group_mask(G));
+                const T inv = pinv[c];
                 const T* U = S + piv[c] * LDS + c0;
                 // multipliers of the unused rows (0 for the others)
                 T l[R];
@@ -449,10 +454,9 @@ __device__ __forceinline__ int eliminate_blocked(T* S, int* piv, int* act, unsig
 // for c = n-1 .. 0 the owner of step c forms x_c = y * (1 / pivot_c) and
 // broadcasts it by shuffle, and the rows pivoted before c update with
 // u(row, c). The owner keeps x_c: xs[sl][q] of lane l is component
-// l + G*sl. With TOX, X[c*NRHS + q] also receives x_c. Each lane forms
-// 1 / pivot of its own steps from the pivots in S (the same rounding as
-// the elimination's), and `after_loads` runs once the pivot order has been
-// read (it may reuse the bookkeeping slots). Steps below `cstop` are not
+// l + G*sl. With TOX, X[c*NRHS + q] also receives x_c. Each lane reads
+// 1 / pivot of its own steps up front, and `after_loads` runs once the pivot
+// order has been read (it may reuse the bookkeeping slots). Steps below `cstop` are not
 // taken: x_c depends only on the x of later steps, so a caller that needs
 // the unknowns cstop .. n-1 alone (the weights, after the polynomial
 // multipliers) gets them unchanged.
@@ -460,7 +464,8 @@ struct NoHook {
     __device__ void operator()() const {}
 };
 template <typename T, int R, int LDS, int NRHS, int G = 32, bool TOX = true, class Hook = NoHook>
-__device__ __forceinline__ void back_substitute_blk(const T* S, const int* piv, T* X, int n,
+__device__ __forceinline__ void back_substitute_blk(const T* S, const int* piv, const T* pinv,
+                                                    T* X, int n,
                                                     int lane, T (&xs)[R][NRHS],
                                                     Hook after_loads = Hook{}, int cstop = 0) {
     const unsigned FULL = group_mask(G);
@@ -477,7 +482,7 @@ __device__ __forceinline__ void back_substitute_blk(const T* S, const int* piv, 
         prow_t[sl] = t < n ? piv[t] : 0;
 #pragma unroll
         for (int q = 0; q < NRHS; ++q) y[sl][q] = t < n ? S[prow_t[sl] * LDS + n + q] : T(0);
-        dvown[sl] = t < n ? recip_rn(S[prow_t[sl] * LDS + t]) : T(0);
+        dvown[sl] = t < n ? pinv[t] : T(0);
     }
     __syncwarp(group_mask(G));
     after_loads();
@@ -733,7 +738,8 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
     }
     __syncwarp(group_mask(G));
 
-    const int info = eliminate_blocked<T, R, LDS, NRHS, PB, G>(S, piv, act, alive, n, lane);
+    T* pinv = reinterpret_cast<T*>(smem + C::off_pinv);
+    const int info = eliminate_blocked<T, R, LDS, NRHS, PB, G>(S, pinv, piv, act, alive, n, lane);
 
     // prefetch stage 3: the next stencil's neighbour coordinates into cx/cy,
     // once the back substitution has read the pivot order: every lane reads
@@ -765,7 +771,7 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
     T xs[R][NRHS];
     // the FP64 form needs the weights alone (unknowns NP .. n-1); the refined
     // form's residual needs every unknown
-    back_substitute_blk<T, R, LDS, NRHS, G, MIXED>(S, piv, X, n, lane, xs, stage3,
+    back_substitute_blk<T, R, LDS, NRHS, G, MIXED>(S, piv, pinv, X, n, lane, xs, stage3,
                                                    MIXED ? 0 : NP);
     if constexpr (!MIXED) {
         scatter_regs<T, R, NRHS, G>(p, xs, NP, ks, off, e, info, s, lane);
@@ -784,7 +790,7 @@ __device__ __forceinline__ void assemble_blk(const AsmParams& p, int s, int sn, 
             ++sweeps;
             residual_blk<T, LDS, NRHS, NP, G>(S, phi, pm, x64, b64, ks, lane);
             forward_substitute_blk<T, R, LDS, NRHS, G>(S, piv, n, lane);
-            back_substitute_blk<T, R, LDS, NRHS, G, true>(S, piv, X, n, lane, xs);
+            back_substitute_blk<T, R, LDS, NRHS, G, true>(S, piv, pinv, X, n, lane, xs);
             // x += d; convergence on max|d| / max|x| per right-hand side
             float worst = 0.f;
             for (int q = 0; q < p.nrhs; ++q) {
@@ -966,9 +972,10 @@ __device__ __forceinline__ void assemble_any(const AsmParams& p, int s, int off,
         default: fill_system_q<T, LDS, NRHS, 4>(p, Q, S, cx, cy, ks, e, lane); break;
     }
     __syncwarp(group_mask(G));
-    const int info = eliminate_blocked<T, L::R, LDS, NRHS, PB>(S, piv, act, alive, n, lane);
+    T* pinv = reinterpret_cast<T*>(base + L::off_pinv);
+    const int info = eliminate_blocked<T, L::R, LDS, NRHS, PB>(S, pinv, piv, act, alive, n, lane);
     T xs[L::R][NRHS];
-    back_substitute_blk<T, L::R, LDS, NRHS, G, false>(S, piv, nullptr, n, lane, xs, NoHook{}, np);
+    back_substitute_blk<T, L::R, LDS, NRHS, G, false>(S, piv, pinv, nullptr, n, lane, xs, NoHook{}, np);
     scatter_regs<T, L::R, NRHS, G>(p, xs, np, ks, off, e, info, s, lane);
 }
 

@@ -20,7 +20,6 @@
 RBFB_VARIANT(f64_p4q7_n64_smem, double, 16, 2, 64, 3, 4, 7, false, 32, 1, true, true)
 RBFB_VARIANT(f64_p4q7_n80_smem, double, 16, 2, 80, 3, 4, 7, false, 32, 1, true, true)
 RBFB_BLK_VARIANT(b64_p3q5_n45_pb8, double, 45, 3, 3, 5, false, 32, 1, 8, true)
-RBFB_BLK_VARIANT(b64_p3q5_n45_pb8x2, double, 45, 3, 3, 5, false, 64, 6, 8, true)
 RBFB_BLK_VARIANT(b64_p3q5_n45_pb8x3, double, 45, 3, 3, 5, false, 96, 4, 8, true)
 RBFB_BLK16_VARIANT(b64_p3q5_n45_pb8_h1, double, 45, 3, 3, 5, false, 32, 1, 8, true)
 RBFB_BLK_VARIANT(b64_p3q5_n48_pb8, double, 48, 3, 3, 5, false, 32, 1, 8, true)
