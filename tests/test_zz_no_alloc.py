@@ -5,12 +5,14 @@ It is meant for callers that may not allocate device memory while running
 another allocator). Checked here through the C ABI against the ordinary
 entry point rbfb_knn_stencils: the stencils are integer indices, so the two
 must agree exactly, and they must keep agreeing on a second call in a row
-(the fixed scratch keeps the previous call's contents). This file is named
-to be collected last.
+(the fixed scratch keeps the previous call's contents). On a tie-free
+non-uniform cloud it is also checked on its own against the oracle's
+brute-force search. This file is named to be collected last.
 """
 import numpy as np
 import pytest
 
+import oracle as O
 import rbf_b200 as R
 from rbf_b200 import nodesets as NS
 
@@ -41,6 +43,21 @@ def test_static_search_matches_the_ordinary_one(torch_cuda):
                 T.cuda.synchronize()
                 np.testing.assert_array_equal(ja.cpu().numpy(), ref.cpu().numpy(),
                                               err_msg=f"call {call}, n={n}, k={k}")
+
+
+def test_static_search_against_the_oracle(torch_cuda):
+    """Gaussian-bump density (a 4x range of spacings, so the fixed cell grid
+    holds crowded and sparse cells), k = 64 and k = 21: index-exact against
+    the oracle's brute force, with the completion status read back."""
+    T = torch_cuda
+    x, y, _ = NS.gaussian_bump(6000, seed=11)
+    xd, yd = T.as_tensor(x).cuda(), T.as_tensor(y).cuda()
+    for k in (64, 21):
+        ja = T.full((x.size * k,), -1, dtype=T.int32, device="cuda")
+        R.knn_stencils_static(xd, yd, k, ja)
+        assert R.knn_static_status() == 0
+        T.cuda.synchronize()
+        np.testing.assert_array_equal(ja.cpu().numpy(), O.knn_brute(x, y, k), err_msg=f"k={k}")
 
 
 def test_static_search_rejects_oversize(torch_cuda):
