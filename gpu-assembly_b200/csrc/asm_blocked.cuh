@@ -147,6 +147,37 @@ __device__ __forceinline__ uint32_t hiword(double v) {
 }
 __device__ __forceinline__ uint32_t hiword(float v) { return __float_as_uint(v); }
 
+// c0, c1 -= m * (b0, b1): one packed FP32 fused multiply-add of sm_100a
+// (fma.rn.f32x2; each component rounded once, as fmaf).
+__device__ __forceinline__ void fnma2(float m, float b0, float b1, float& c0, float& c1) {
+    unsigned long long mm, bb, cc, d;
+    const float nm = -m;
+    asm("mov.b64 %0, {%1, %1};" : "=l"(mm) : "f"(nm));
+    asm("mov.b64 %0, {%1, %2};" : "=l"(bb) : "f"(b0), "f"(b1));
+    asm("mov.b64 %0, {%1, %2};" : "=l"(cc) : "f"(c0), "f"(c1));
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(mm), "l"(bb), "l"(cc));
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(c0), "=f"(c1) : "l"(d));
+}
+
+// c[j] = fma(-m, b[j], c[j]) for j0 <= j < END: FP64 one fused multiply-add
+// each; FP32 in aligned pairs through fnma2.
+template <int END>
+__device__ __forceinline__ void fnma_range(double m, const double* b, double* c, int j0) {
+#pragma unroll
+    for (int j = j0; j < END; ++j) c[j] = fma(-m, b[j], c[j]);
+}
+template <int END>
+__device__ __forceinline__ void fnma_range(float m, const float* b, float* c, int j0) {
+    int j = j0;
+    if (j & 1) {
+        if (j < END) c[j] = fmaf(-m, b[j], c[j]);
+        ++j;
+    }
+#pragma unroll
+    for (; j + 1 < END; j += 2) fnma2(m, b[j], b[j + 1], c[j], c[j + 1]);
+    if (j < END) c[j] = fmaf(-m, b[j], c[j]);
+}
+
 // ---- the phases of one stencil, shared by the fixed-shape and the uneven
 // kernels. A stencil's working set (S, X, pinv, piv, act, alive, cx, cy) is
 // in shared memory, or -- for the uneven kernel's large stencils -- in a
@@ -375,9 +406,7 @@ __device__ __forceinline__ int eliminate_blocked(T* S, T* pinv, int* piv, int* a
                         mk_next = __reduce_max_sync(FULL, pkey);
                     }
 #pragma unroll
-                    for (int j = t + 2; j < PB; ++j)
-#pragma unroll
-                        for (int sl = 0; sl < R; ++sl) a[sl][j] = fma(-l[sl], u[j], a[sl][j]);
+                    for (int sl = 0; sl < R; ++sl) fnma_range<PB>(l[sl], u, a[sl], t + 2);
                 }
             }
         }
@@ -408,8 +437,7 @@ __device__ __forceinline__ int eliminate_blocked(T* S, T* pinv, int* piv, int* a
 #pragma unroll
                     for (int tp = 0; tp < t; ++tp) {
                         const T lv = S[prw[t] * LDS + c0 + tp];
-#pragma unroll
-                        for (int q = 0; q < VE; ++q) u[t][q] = fma(-lv, u[tp][q], u[t][q]);
+                        fnma_range<VE>(lv, u[tp], u[t], 0);
                     }
                     stv(S + prw[t] * LDS + col, u[t]);
                 }
@@ -436,9 +464,7 @@ __device__ __forceinline__ int eliminate_blocked(T* S, T* pinv, int* piv, int* a
                         T cv[VE];
                         ldv(cp, cv);
 #pragma unroll
-                        for (int t = 0; t < PB; ++t)
-#pragma unroll
-                            for (int q = 0; q < VE; ++q) cv[q] = fma(-a[sl][t], u[t][q], cv[q]);
+                        for (int t = 0; t < PB; ++t) fnma_range<VE>(a[sl][t], u[t], cv, 0);
                         if (kmask[sl]) stv(cp, cv);
                     }
                 }
