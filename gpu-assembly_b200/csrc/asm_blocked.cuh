@@ -549,8 +549,7 @@ __device__ __forceinline__ void back_substitute_blk(const T* S, const int* piv, 
 #pragma unroll
             for (int sl = 0; sl <= OS; ++sl) {
                 const T u = (sl == OS && lane + G * sl >= c) ? T(0) : uc[sl];
-#pragma unroll
-                for (int q = 0; q < NRHS; ++q) y[sl][q] = fma(-u, xq[q], y[sl][q]);
+                fnma_range<NRHS>(u, xq, y[sl], 0);
             }
         }
     };
@@ -592,8 +591,7 @@ __device__ __forceinline__ void forward_substitute_blk(T* S, const int* piv, int
             for (int sl = OS; sl < R; ++sl) {
                 T l = S[prow_t[sl] * LDS + c];
                 if (sl == OS) l = (lane + G * sl > c) ? l : T(0);
-#pragma unroll
-                for (int q = 0; q < NRHS; ++q) y[sl][q] = fma(-l, z[q], y[sl][q]);
+                fnma_range<NRHS>(l, z, y[sl], 0);
             }
         }
     };
