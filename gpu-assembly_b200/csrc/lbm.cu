@@ -17,15 +17,15 @@
 // of the post-collision field f_a at the departure point x_s - c_a dt,
 // sum_j W_a[s*k + j] * f_a[ja[s*k + j]], with W_a the weights of the
 // interpolation right-hand side at that point (rbfb_assemble with
-// RBFB_OP_INTERP and the 8 departure points). One warp takes 32 consecutive
-// nodes: for each node, lane j multiplies entry j (and adds entry j + 32 by a
-// fused multiply-add when k > 32), an xor butterfly sums the lanes, and the
-// node's lane keeps the result; then every lane collides its own node and the
-// warp writes 32 consecutive entries of each direction. The oracle restates
-// that summation order.
+// RBFB_OP_INTERP and the 8 departure points). The sum runs in entry order,
+// j = 0 first: the first product rounded, then one fused multiply-add an
+// entry, as a CSR row product does. A warp stages 32 nodes' rows in shared
+// memory and each lane sums its own node's row; the oracle restates that
+// order.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdint>
 
 #include "rbf_b200.h"
 
@@ -187,57 +187,217 @@ __global__ void bgk_kernel(int n, T omega, T* __restrict__ pdf, T* __restrict__ 
     }
 }
 
+// Streamed data (weights, indices) is read once per step: an L2 policy that
+// evicts it first keeps the gathered field pdf_in resident in L2 while the
+// weights, about 18 times its size, pass through.
+__device__ __forceinline__ unsigned long long evict_first_policy() {
+    unsigned long long pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;\n" : "=l"(pol));
+    return pol;
+}
+template <int BYTES>
+__device__ __forceinline__ void cp_async_stream(void* dst, const void* src,
+                                                unsigned long long pol) {
+    if constexpr (BYTES == 16)  // .cg: to shared memory through L2 only
+        asm volatile("cp.async.cg.shared.global.L2::cache_hint [%0], [%1], 16, %2;\n" ::"r"(
+                         (unsigned)__cvta_generic_to_shared(dst)),
+                     "l"(src), "l"(pol)
+                     : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global.L2::cache_hint [%0], [%1], %2, %3;\n" ::"r"(
+                         (unsigned)__cvta_generic_to_shared(dst)),
+                     "l"(src), "n"(BYTES), "l"(pol)
+                     : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int PENDING>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(PENDING) : "memory");
+}
+// Waits until at most `pending` (0..3; a constant once the caller's loop is
+// unrolled) of this thread's copy groups are still in flight.
+__device__ __forceinline__ void cp_async_wait_pending(int pending) {
+    switch (pending) {
+        case 0: cp_async_wait<0>(); break;
+        case 1: cp_async_wait<1>(); break;
+        case 2: cp_async_wait<2>(); break;
+        default: cp_async_wait<3>(); break;
+    }
+}
+
+constexpr int kTileWarps = 4;  // warps a CTA; each warp owns a 32-node tile at a time
+
+// Shared memory of one warp: DEPTH weight slabs (the directions in flight)
+// and the tile's index slab, 32 rows of ks entries each; ks = k for odd k,
+// k + 1 for even k, so that row r of lane r is bank-conflict free.
+inline int tile_stride(int k) { return (k & 1) ? k : k + 1; }
+inline size_t tile_smem_bytes(int k, int depth) {
+    return static_cast<size_t>(kTileWarps) * 32 * tile_stride(k) *
+           (depth * sizeof(double) + sizeof(int));
+}
+
+// Copies the tile's m = cnt * k consecutive entries (element e to row e / k,
+// column e % k of a ks-strided slab); lane takes e = lane + 32 i. (r, c) is
+// the row and column of the lane's current element, advanced by 32 entries.
+// VEC (unpadded slabs, 16-byte aligned source and destination): 16-byte
+// copies, the odd tail entries one by one.
+template <bool PAD, bool VEC, typename V>
+__device__ __forceinline__ void copy_slab(V* dst, const V* src, int m, int k, int ks, int lane,
+                                          int r, int c, int q32, int r32,
+                                          unsigned long long pol) {
+    if constexpr (VEC && !PAD) {
+        constexpr int per = 16 / sizeof(V);
+        const int chunks = m / per;
+        for (int q = lane; q < chunks; q += 32)
+            cp_async_stream<16>(dst + q * per, src + q * per, pol);
+        for (int e = chunks * per + lane; e < m; e += 32)
+            cp_async_stream<sizeof(V)>(dst + e, src + e, pol);
+    } else {
+        for (int e = lane; e < m; e += 32) {
+            cp_async_stream<sizeof(V)>(dst + (PAD ? r * ks + c : e), src + e, pol);
+            if (PAD) {
+                r += q32;
+                c += r32;
+                if (c >= k) {
+                    c -= k;
+                    ++r;
+                }
+            }
+        }
+    }
+}
+
 // Semi-Lagrangian streaming of the post-collision field pdf_in through the
 // interpolation operators W (8 arrays of n*k weights, direction a at
 // W + (a-1)*n*k, rows like ja), then the BGK collision, into pdf_out. The
 // moments of the streamed populations go to rho, ux, uy (any may be null).
-template <typename T>
-__global__ void __launch_bounds__(256) stream_collide_kernel(int n, int k,
-                                                             const int* __restrict__ ja,
-                                                             const double* __restrict__ W,
-                                                             T omega, const T* __restrict__ pdf_in,
-                                                             T* __restrict__ pdf_out,
-                                                             T* __restrict__ rho,
-                                                             T* __restrict__ ux,
-                                                             T* __restrict__ uy) {
-    const int lane = threadIdx.x & 31;
+// A warp takes a tile of 32 consecutive nodes: it copies the tile's index
+// rows and the first DEPTH - 1 directions' weight rows into shared memory;
+// for each direction it starts the copy of the direction DEPTH - 1 ahead and
+// has each lane sum its own node's row in entry order (the first product
+// rounded, then one fused multiply-add an entry), gathering pdf_in through
+// the indices. Then every lane collides its node and the warp writes 32
+// consecutive entries of each direction, as streaming stores. KT > 0 fixes
+// k at compile time (the row's gathers all in flight at once).
+template <typename T, bool PAD, int KT, int DEPTH, bool VEC>
+__global__ void __launch_bounds__(kTileWarps * 32) stream_collide_kernel(
+    int n, int k, const int* __restrict__ ja, const double* __restrict__ W, T omega,
+    const T* __restrict__ pdf_in, T* __restrict__ pdf_out, T* __restrict__ rho,
+    T* __restrict__ ux, T* __restrict__ uy) {
+    static_assert(DEPTH >= 2 && DEPTH <= 4, "prefetch depth");
+    extern __shared__ __align__(16) unsigned char tile_smem[];
+    if (KT > 0) k = KT;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const int ks = PAD ? k + 1 : k;
+    const int slab = 32 * ks;
+    double* wbuf =
+        reinterpret_cast<double*>(tile_smem) + static_cast<size_t>(wid) * DEPTH * slab;
+    int* jbuf = reinterpret_cast<int*>(reinterpret_cast<double*>(tile_smem) +
+                                       static_cast<size_t>(kTileWarps) * DEPTH * slab) +
+                static_cast<size_t>(wid) * slab;
     const size_t N = static_cast<size_t>(n);
     const size_t nnz = N * static_cast<size_t>(k);
-    const int warps = (gridDim.x * blockDim.x) >> 5;
-    for (int s0 = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; s0 < n; s0 += warps * 32) {
-        T mine[9];
-#pragma unroll
-        for (int a = 0; a < 9; ++a) mine[a] = T(0);
+    const unsigned long long pol = evict_first_policy();
+    const int r0 = lane / k, c0 = lane - r0 * k, q32 = 32 / k, r32 = 32 - q32 * k;
+    const int tiles = (n + 31) >> 5;
+    for (int tile = blockIdx.x * kTileWarps + wid; tile < tiles; tile += gridDim.x * kTileWarps) {
+        const int s0 = tile << 5;
         const int cnt = min(32, n - s0);
-        for (int t = 0; t < cnt; ++t) {
-            const int s = s0 + t;
-            const size_t row = static_cast<size_t>(s) * k;
-            const bool has0 = lane < k, has1 = lane + 32 < k;
-            const int j0 = has0 ? ja[row + lane] : 0;
-            const int j1 = has1 ? ja[row + lane + 32] : 0;
+        const int m = cnt * k;
+        const size_t base = static_cast<size_t>(s0) * k;
+        copy_slab<PAD, VEC>(jbuf, ja + base, m, k, ks, lane, r0, c0, q32, r32, pol);
 #pragma unroll
-            for (int a = 1; a < 9; ++a) {
-                const double* Wa = W + static_cast<size_t>(a - 1) * nnz + row;
-                T v = T(0);
-                if (has0) v = mul(static_cast<T>(Wa[lane]), pdf_in[j0 + N * a]);
-                if (has1) v = fmaT(static_cast<T>(Wa[lane + 32]), pdf_in[j1 + N * a], v);
+        for (int d = 1; d < DEPTH; ++d) {
+            copy_slab<PAD, VEC>(wbuf + (d - 1) * slab, W + static_cast<size_t>(d - 1) * nnz + base,
+                                m, k, ks, lane, r0, c0, q32, r32, pol);
+            cp_async_commit();
+        }
+        T f[9];
 #pragma unroll
-                for (int o = 16; o > 0; o >>= 1) v = add(v, __shfl_xor_sync(0xffffffffu, v, o));
-                if (lane == t) mine[a] = v;
+        for (int a = 1; a < 9; ++a) {
+            const int nxt = a + DEPTH - 1;  // the direction whose copy starts now
+            if (nxt <= 8) {
+                copy_slab<PAD, VEC>(wbuf + ((nxt - 1) % DEPTH) * slab,
+                                    W + static_cast<size_t>(nxt - 1) * nnz + base, m, k, ks, lane,
+                                    r0, c0, q32, r32, pol);
+                cp_async_commit();
             }
+            cp_async_wait_pending(min(DEPTH - 1, 8 - a));
+            __syncwarp();
+            if (lane < cnt) {
+                const double* wr = wbuf + ((a - 1) % DEPTH) * slab + lane * ks;
+                const int* jr = jbuf + lane * ks;
+                const T* pa = pdf_in + N * a;
+                T v = mul(static_cast<T>(wr[0]), pa[jr[0]]);
+                if constexpr (KT > 0) {
+#pragma unroll
+                    for (int j = 1; j < KT; ++j) v = fmaT(static_cast<T>(wr[j]), pa[jr[j]], v);
+                } else {
+#pragma unroll 8
+                    for (int j = 1; j < k; ++j) v = fmaT(static_cast<T>(wr[j]), pa[jr[j]], v);
+                }
+                f[a] = v;
+            }
+            __syncwarp();  // every lane is done with this buffer before it is refilled
         }
         const int s = s0 + lane;
         if (lane < cnt) {
-            mine[0] = pdf_in[s];  // the rest population does not move
+            f[0] = pdf_in[s];  // the rest population does not move
             T o[9], r, u, v, d;
-            collide(mine, omega, o, r, u, v, d);
+            collide(f, omega, o, r, u, v, d);
 #pragma unroll
-            for (int a = 0; a < 9; ++a) pdf_out[s + N * a] = o[a];
-            if (rho) rho[s] = r;
-            if (ux) ux[s] = u;
-            if (uy) uy[s] = v;
+            for (int a = 0; a < 9; ++a) __stcs(pdf_out + s + N * a, o[a]);
+            if (rho) __stcs(rho + s, r);
+            if (ux) __stcs(ux + s, u);
+            if (uy) __stcs(uy + s, v);
         }
     }
+}
+
+template <typename T, bool PAD, int KT, int DEPTH, bool VEC>
+int launch_stream_collide(int n, int k, const int* ja, const double* W, T omega, const T* pin,
+                          T* pout, T* rho, T* ux, T* uy, cudaStream_t st) {
+    auto kern = stream_collide_kernel<T, PAD, KT, DEPTH, VEC>;
+    const size_t smem = tile_smem_bytes(k, DEPTH);
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem)) != cudaSuccess)
+        return RBFB_ECUDA;
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kTileWarps * 32, smem) !=
+            cudaSuccess ||
+        per_sm < 1)
+        return RBFB_ECUDA;
+    const int tiles = (n + 31) / 32;
+    const int blocks = std::max(1, std::min((tiles + kTileWarps - 1) / kTileWarps,
+                                            std::max(sms, 1) * per_sm));
+    kern<<<blocks, kTileWarps * 32, smem, st>>>(n, k, ja, W, omega, pin, pout, rho, ux, uy);
+    return cudaGetLastError() == cudaSuccess ? RBFB_OK : RBFB_ECUDA;
+}
+
+template <typename T>
+int stream_collide(int n, int k, const int* ja, const double* W, T omega, const T* pin, T* pout,
+                   T* rho, T* ux, T* uy, cudaStream_t st) {
+    // 16-byte copies need 16-byte aligned rows: ja, W and every direction's
+    // array (n*k even). Odd k: unpadded slabs; k = 21 (the D2Q9 operators'
+    // usual stencil) fixed at compile time. Even k: padded slabs, 8-byte
+    // copies.
+    const bool vec = ((reinterpret_cast<uintptr_t>(ja) | reinterpret_cast<uintptr_t>(W)) & 15) == 0 &&
+                     ((static_cast<long long>(n) * k) & 1) == 0;
+    if (!(k & 1))
+        return launch_stream_collide<T, true, 0, 2, false>(n, k, ja, W, omega, pin, pout, rho, ux,
+                                                           uy, st);
+    if (vec && k == 21)
+        return launch_stream_collide<T, false, 21, 2, true>(n, k, ja, W, omega, pin, pout, rho,
+                                                            ux, uy, st);
+    if (vec)
+        return launch_stream_collide<T, false, 0, 2, true>(n, k, ja, W, omega, pin, pout, rho, ux,
+                                                           uy, st);
+    return launch_stream_collide<T, false, 0, 2, false>(n, k, ja, W, omega, pin, pout, rho, ux,
+                                                        uy, st);
 }
 
 int blocks_for(int n) {
@@ -315,19 +475,16 @@ int rbfb_lbm_stream_collide(int n, int precision, int k, const int* ja, const do
         return RBFB_EINVAL;
     if (n == 0) return RBFB_OK;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    const int blocks = std::max(1, std::min((n + 255) / 256, 148 * 16));
     if (precision == RBFB_FP64)
-        stream_collide_kernel<double><<<blocks, 256, 0, st>>>(
-            n, k, ja, W, omega, static_cast<const double*>(pdf_in), static_cast<double*>(pdf_out),
-            static_cast<double*>(rho), static_cast<double*>(ux), static_cast<double*>(uy));
-    else if (precision == RBFB_LBM_FP32)
-        stream_collide_kernel<float><<<blocks, 256, 0, st>>>(
-            n, k, ja, W, static_cast<float>(omega), static_cast<const float*>(pdf_in),
-            static_cast<float*>(pdf_out), static_cast<float*>(rho), static_cast<float*>(ux),
-            static_cast<float*>(uy));
-    else
-        return RBFB_EINVAL;
-    return cudaGetLastError() == cudaSuccess ? RBFB_OK : RBFB_ECUDA;
+        return stream_collide<double>(n, k, ja, W, omega, static_cast<const double*>(pdf_in),
+                                      static_cast<double*>(pdf_out), static_cast<double*>(rho),
+                                      static_cast<double*>(ux), static_cast<double*>(uy), st);
+    if (precision == RBFB_LBM_FP32)
+        return stream_collide<float>(n, k, ja, W, static_cast<float>(omega),
+                                     static_cast<const float*>(pdf_in),
+                                     static_cast<float*>(pdf_out), static_cast<float*>(rho),
+                                     static_cast<float*>(ux), static_cast<float*>(uy), st);
+    return RBFB_EINVAL;
 }
 
 }  // extern "C"

@@ -9,6 +9,7 @@ reference's assembly, as the parity tests establish).
     python -m rbf_b200.run --workload disk --precision both
     python -m rbf_b200.run --workload bump --precision both
     python -m rbf_b200.run --workload disk --precision fp64 --solve 200
+    python -m rbf_b200.run --workload lbm --grid 1024 --reps 20
 
 Workloads:
   periodic  jittered m x m grid in the periodic unit square (m = --grid),
@@ -18,6 +19,10 @@ Workloads:
             2/3: ragged CSR stencils, bucketed by system size, graph-replayed
   bump      2,097,152 nodes with a 4x Gaussian-bump density, k=64, PHS r^7 +
             degree 4 (n=79)
+  lbm       D2Q9 semi-Lagrangian lattice Boltzmann on the periodic m x m grid:
+            FP64 interpolation operators (k=21, PHS r^3 + degree 2) at the 8
+            departure points x - c_a h/2, assembled once, then --reps fused
+            stream + collide steps (populations in --populations precision)
 The single-kernel shapes are also what the profiles are captured on (e.g.
 under ncu with ``-k regex:asm_kernel`` on ``--grid 512``).
 
@@ -105,13 +110,62 @@ def disk_csr(ctx, dev, n=None):
                 kmax=kmax)
 
 
+def lbm(ctx, dev, stream, a):
+    """The lattice Boltzmann workload: operators assembled once, then a.reps
+    fused stream + collide steps ping-ponging two population arrays. Device
+    time per step (CUDA events over all steps, after 3 warm-up steps) and the
+    algorithmic bytes per node over it."""
+    m, k, P = a.grid, a.k or 21, a.degree or 2
+    x, y, _ = NS.jittered_grid(m, 0.3, seed=2, periodic=True)
+    n = x.size
+    xd, yd = torch.as_tensor(x, device=dev), torch.as_tensor(y, device=dev)
+    ja = torch.empty(n * k, dtype=torch.int32, device=dev)
+    ctx.knn_stencils(xd, yd, k, ja, period=(1.0, 1.0))
+    xc, yc = R.lbm_departure_points(0.5 / m)
+    xcd, ycd = torch.as_tensor(xc, device=dev), torch.as_tensor(yc, device=dev)
+    W = torch.empty(8 * n * k, dtype=torch.float64, device=dev)
+    vals = [W[i * n * k:(i + 1) * n * k] for i in range(8)]
+    d = R.make_desc(P, 0, R.OP_INTERP, R.FP64, True, period=(1.0, 1.0), xc=xcd, yc=ycd, nc=8)
+    st = ctx.assemble(d, xd, yd, k, ja, vals, stats=True)
+    dt = torch.float64 if a.populations == "fp64" else torch.float32
+    rho = torch.as_tensor(1.0 + 0.02 * np.sin(2 * np.pi * x), dtype=dt, device=dev)
+    ux = torch.as_tensor(0.03 * np.cos(2 * np.pi * y), dtype=dt, device=dev)
+    uy = torch.as_tensor(0.01 * np.sin(2 * np.pi * (x + y)), dtype=dt, device=dev)
+    bufs = [torch.empty(9 * n, dtype=dt, device=dev) for _ in range(2)]
+    R.lbm_feq(rho, ux, uy, bufs[0])
+    torch.cuda.synchronize()
+
+    def step(i):
+        R.lbm_stream_collide(k, ja, W, 1.5, bufs[i % 2], bufs[(i + 1) % 2], rho, ux, uy,
+                             stream=stream)
+    for i in range(3):
+        step(i)
+    ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ea.record(stream)
+    for i in range(a.reps):
+        step(i)
+    eb.record(stream)
+    torch.cuda.synchronize()
+    ms = ea.elapsed_time(eb) / max(a.reps, 1)
+    es = dt.itemsize
+    per_node = 8 * k * 8 + 4 * k + 2 * 9 * es + 3 * es
+    return {"nodes": n, "k": k, "degree": P, "populations": a.populations,
+            "operator_assembly_ms": st["ms"], "ms_per_step": ms,
+            "node_updates_per_s": n / (ms * 1e-3), "bytes_per_node": per_node,
+            "algorithmic_GBps": per_node * n / (ms * 1e-3) / 1e9}
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", choices=["periodic", "disk", "bump"], default="periodic")
+    ap.add_argument("--workload", choices=["periodic", "disk", "bump", "lbm"],
+                    default="periodic")
     ap.add_argument("--grid", type=int, default=256, help="periodic: grid side")
     ap.add_argument("--n", type=int, default=None, help="disk/bump: number of nodes")
-    ap.add_argument("--k", type=int, default=35)
-    ap.add_argument("--degree", type=int, default=3)
+    ap.add_argument("--k", type=int, default=None, help="periodic: 35, lbm: 21")
+    ap.add_argument("--degree", type=int, default=None, help="periodic: 3, lbm: 2")
+    ap.add_argument("--populations", choices=["fp64", "fp32"], default="fp64",
+                    help="lbm: precision of the populations")
     ap.add_argument("--precision", choices=["fp64", "mixed", "both"], default="mixed")
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--tune", action="store_true", help="autotune the shape first")
@@ -128,7 +182,9 @@ def main(argv=None):
     out = {"workload": a.workload}
 
     with R.Context(0) as ctx:
-        if a.workload == "disk":
+        if a.workload == "lbm":
+            out.update(lbm(ctx, dev, stream, a))
+        elif a.workload == "disk":
             w = disk_csr(ctx, dev, a.n)
             c, xd, yd, ia, ja, deg = w["c"], w["xd"], w["yd"], w["ia"], w["ja"], w["deg"]
             kvec = w["kvec"]
@@ -178,7 +234,7 @@ def main(argv=None):
                 k, P, per = c["k"], c["P"], None
             else:
                 x, y, _ = NS.jittered_grid(a.grid, 0.3, seed=2, periodic=True)
-                k, P, per = a.k, a.degree, (1.0, 1.0)
+                k, P, per = a.k or 35, a.degree or 3, (1.0, 1.0)
             n = x.size
             xd, yd = torch.as_tensor(x, device=dev), torch.as_tensor(y, device=dev)
             ja = torch.empty(n * k, dtype=torch.int32, device=dev)

@@ -323,7 +323,8 @@ int rbfb_lbm_bgk(int n, int precision, double omega, void* pdf, void* rho, void*
 /* One semi-Lagrangian time step: streaming of the post-collision field
  * pdf_in through the interpolation operators, then the BGK collision, into
  * pdf_out (must not alias pdf_in). Direction a (1..8) of node s becomes
- * sum_j W[(a-1)*n*k + s*k + j] * pdf_in[ja[s*k + j] + n*a] -- the weights of
+ * sum_j W[(a-1)*n*k + s*k + j] * pdf_in[ja[s*k + j] + n*a], summed in j
+ * order (the j = 0 product rounded, then a fused multiply-add per entry) -- the weights of
  * interpolation at the departure point x_s - c_a dt, as rbfb_assemble
  * returns them for RBFB_OP_INTERP at those 8 points (W: 8 consecutive arrays
  * of n*k doubles, FP64; rounded to float for RBFB_LBM_FP32); the rest

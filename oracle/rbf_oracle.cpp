@@ -974,9 +974,8 @@ extern "C" int orc_bicgstab(int n, int k, const int* ia, const int* ja, const do
 // -ffp-contract=off). Planar storage, direction a of node i at pdf[i + n*a].
 // The streaming step (which the reference does not ship) sums the
 // interpolation weights times the gathered populations in the order the CUDA
-// kernel does: lane j of a warp forms w_j * f_j (j < k) and adds w_{j+32} *
-// f_{j+32} with a fused multiply-add (j + 32 < k); an xor butterfly over 32
-// lanes (offsets 16, 8, 4, 2, 1) adds the lanes.
+// kernel does: in entry order, w_0 * f_0 rounded, then one fused
+// multiply-add per entry j = 1 .. k-1.
 namespace lbm {
 
 template <typename T>
@@ -1093,19 +1092,10 @@ void stream_collide(int n, int k, const int* ja, const double* W, T omega, const
         f[0] = pin[s];
         for (int a = 1; a < 9; ++a) {
             const double* Wa = W + static_cast<size_t>(a - 1) * nnz + row;
-            T v[32];
-            for (int l = 0; l < 32; ++l) {
-                T t = T(0);
-                if (l < k) t = static_cast<T>(Wa[l]) * pin[ja[row + l] + N * a];
-                if (l + 32 < k) t = fma_t(static_cast<T>(Wa[l + 32]), pin[ja[row + l + 32] + N * a], t);
-                v[l] = t;
-            }
-            for (int o = 16; o > 0; o >>= 1) {
-                T w[32];
-                for (int l = 0; l < 32; ++l) w[l] = v[l] + v[l ^ o];
-                for (int l = 0; l < 32; ++l) v[l] = w[l];
-            }
-            f[a] = v[0];
+            const T* pa = pin + N * a;
+            T v = static_cast<T>(Wa[0]) * pa[ja[row]];
+            for (int j = 1; j < k; ++j) v = fma_t(static_cast<T>(Wa[j]), pa[ja[row + j]], v);
+            f[a] = v;
         }
         T o[9], r, u, w, d;
         collide(f, omega, o, &r, &u, &w, &d);

@@ -7,8 +7,9 @@
   program, a process of its own.
 * the fused streaming + collision step through interpolation operators
   assembled by this library at the 8 departure points x_s - c_a dt: bit-
-  identical to the oracle's restatement of its summation order; a uniform
-  flow stays uniform.
+  identical to the oracle's restatement of its summation order on every
+  path of the kernel (k = 21 fixed at compile time; other odd k; even k,
+  padded rows; n*k odd, 8-byte copies); a uniform flow stays uniform.
 """
 from pathlib import Path
 
@@ -120,11 +121,14 @@ def _streaming_operators(T, ctx, m=48, k=21, seed=3):
     return ja, W, x, y
 
 
+# (grid side, k): k = 21 with 16-byte copies; n*k odd (47^2 * 21): 8-byte
+# copies; k = 15: odd k not fixed at compile time; k = 16: padded rows
+@pytest.mark.parametrize("mk", [(48, 21), (47, 21), (48, 15), (48, 16)], ids=str)
 @pytest.mark.parametrize("dtype", [np.float64, np.float32])
-def test_stream_collide_matches_oracle(ctx, torch_cuda, dtype):
+def test_stream_collide_matches_oracle(ctx, torch_cuda, dtype, mk):
     T = torch_cuda
-    k = 21
-    ja, W, x, y = _streaming_operators(T, ctx)
+    m, k = mk
+    ja, W, x, y = _streaming_operators(T, ctx, m=m, k=k)
     n = x.size
     rho = (1.0 + 0.02 * np.sin(2 * np.pi * x)).astype(dtype)
     ux = (0.03 * np.cos(2 * np.pi * y)).astype(dtype)
