@@ -16,8 +16,8 @@
 // reads the operator (12 B per stored weight, twice) and a handful of
 // vectors. What holds the operator passes below it is the latency of their
 // gathers (one per stored weight), which each thread hides by summing its
-// own row in row order with eight gathers in flight. It is laid out as five
-// kernels per iteration, each one pass over the rows:
+// own row in row order with eight gathers in flight (row_sum.cuh). It is
+// laid out as five kernels per iteration, each one pass over the rows:
 //   p_kernel       p = r + beta (p - omega v)
 //   spmv_v_kernel  v = A p, with the partial sums of (rh, v)
 //   s_kernel       s = r - alpha v
@@ -45,6 +45,7 @@
 #include <cstring>
 #include <vector>
 
+#include "row_sum.cuh"
 #include "runtime.h"
 
 namespace rbfb {
@@ -69,6 +70,7 @@ struct State {
 
 struct Args {
     int n, k;
+    bool vec;  // ja and values 16-byte aligned: vector loads in row_sum
     const int* ia;
     const int* ja;
     const double* values;
@@ -94,10 +96,7 @@ struct Workspace {
 };
 
 // (A w)_s: row s of the operator applied to the vector w(j), j < n, summed
-// in row order. The loop takes the row eight weights at a time, with the
-// eight weights, columns and gathered entries loaded before the eight fused
-// multiply-adds, so each thread has eight independent gathers in flight
-// instead of one (the sums are the same as a one-at-a-time loop).
+// in row order (row_sum); a boundary row is the identity.
 template <class W>
 __device__ __forceinline__ double apply_row(const Args& a, long long s, W w) {
     if (a.bflag[s]) return w(static_cast<int>(s));
@@ -109,21 +108,7 @@ __device__ __forceinline__ double apply_row(const Args& a, long long s, W w) {
         q = s * a.k;
         e = q + a.k;
     }
-    double acc = 0.0;
-    for (; q + 8 <= e; q += 8) {
-        int j[8];
-        double v[8], x[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) j[i] = __ldg(a.ja + q + i);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) v[i] = __ldg(a.values + q + i);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) x[i] = w(j[i]);
-#pragma unroll
-        for (int i = 0; i < 8; ++i) acc = fma(v[i], x[i], acc);
-    }
-    for (; q < e; ++q) acc = fma(__ldg(a.values + q), w(__ldg(a.ja + q)), acc);
-    return acc;
+    return row_sum(a.ja, a.values, q, e, a.vec, w);
 }
 
 // Sums NV values over the block; the totals end up in every lane of warp 0.
@@ -448,6 +433,7 @@ extern "C" int rbfb_solve_bicgstab(rbfb_ctx* ctx, int n, int k, const int* ia, c
     a.ia = ia;
     a.ja = ja;
     a.values = values;
+    a.vec = rows_vectorizable(ja, values);
     a.bflag = w->bflag;
     a.f = f;
     a.u = u;

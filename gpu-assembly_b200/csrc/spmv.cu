@@ -6,25 +6,23 @@
 //
 // One thread per row, summing its k products in row order with fused
 // multiply-adds from zero: acc = fma(values[s*k+j], u[ja[s*k+j]], acc),
-// j = 0..k-1. The order is pinned so the result is reproducible (the CPU
-// oracle does the same).
+// j = 0..k-1 (row_sum.cuh). The order is pinned so the result is
+// reproducible (the CPU oracle does the same).
 #include <cuda_runtime.h>
 
 #include <algorithm>
 
+#include "row_sum.cuh"
 #include "runtime.h"
 
 namespace rbfb {
 
 __global__ void spmv_fixed_kernel(int n, int k, const int* __restrict__ ja,
                                   const double* __restrict__ values, const double* __restrict__ u,
-                                  double* __restrict__ out) {
+                                  double* __restrict__ out, bool vec) {
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
-        const int* jr = ja + static_cast<size_t>(s) * k;
-        const double* vr = values + static_cast<size_t>(s) * k;
-        double acc = 0.0;
-        for (int j = 0; j < k; ++j) acc = fma(__ldg(vr + j), __ldg(u + __ldg(jr + j)), acc);
-        out[s] = acc;
+        const long long q = static_cast<long long>(s) * k;
+        out[s] = row_sum(ja, values, q, q + k, vec, [u](int j) { return __ldg(u + j); });
     }
 }
 
@@ -44,7 +42,8 @@ extern "C" int rbfb_spmv(int n, int k, const int* ja, const double* values, cons
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (n > 0) {
         const int blocks = std::min((n + 255) / 256, 148 * 16);
-        rbfb::spmv_fixed_kernel<<<blocks, 256, 0, st>>>(n, k, ja, values, u, out);
+        rbfb::spmv_fixed_kernel<<<blocks, 256, 0, st>>>(n, k, ja, values, u, out,
+                                                        rbfb::rows_vectorizable(ja, values));
     }
     if (nbnd > 0) {
         const int blocks = std::min((nbnd + 255) / 256, 148 * 4);
