@@ -233,9 +233,9 @@ constexpr int kTileWarps = 4;  // warps a CTA; each warp owns a 32-node tile at 
 // and the tile's index slab, 32 rows of ks entries each; ks = k for odd k,
 // k + 1 for even k, so that row r of lane r is bank-conflict free.
 inline int tile_stride(int k) { return (k & 1) ? k : k + 1; }
-inline size_t tile_smem_bytes(int k, int depth) {
+inline size_t tile_smem_bytes(int k, int depth, bool jreg) {
     return static_cast<size_t>(kTileWarps) * 32 * tile_stride(k) *
-           (depth * sizeof(double) + sizeof(int));
+           (depth * sizeof(double) + (jreg ? 0 : sizeof(int)));
 }
 
 // Copies the tile's m = cnt * k consecutive entries (element e to row e / k,
@@ -280,13 +280,16 @@ __device__ __forceinline__ void copy_slab(V* dst, const V* src, int m, int k, in
 // rounded, then one fused multiply-add an entry), gathering pdf_in through
 // the indices. Then every lane collides its node and the warp writes 32
 // consecutive entries of each direction, as streaming stores. KT > 0 fixes
-// k at compile time (the row's gathers all in flight at once).
-template <typename T, bool PAD, int KT, int DEPTH, bool VEC>
+// k at compile time (the row's gathers all in flight at once). JREG (with
+// KT): the index rows land in the second weight buffer and each lane keeps
+// its own row in registers for the tile, so no index slab is kept.
+template <typename T, bool PAD, int KT, int DEPTH, bool VEC, bool JREG = false>
 __global__ void __launch_bounds__(kTileWarps * 32) stream_collide_kernel(
     int n, int k, const int* __restrict__ ja, const double* __restrict__ W, T omega,
     const T* __restrict__ pdf_in, T* __restrict__ pdf_out, T* __restrict__ rho,
     T* __restrict__ ux, T* __restrict__ uy) {
     static_assert(DEPTH >= 2 && DEPTH <= 4, "prefetch depth");
+    static_assert(!JREG || (KT > 0 && !PAD && DEPTH == 2), "index rows in registers");
     extern __shared__ __align__(16) unsigned char tile_smem[];
     if (KT > 0) k = KT;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -294,9 +297,10 @@ __global__ void __launch_bounds__(kTileWarps * 32) stream_collide_kernel(
     const int slab = 32 * ks;
     double* wbuf =
         reinterpret_cast<double*>(tile_smem) + static_cast<size_t>(wid) * DEPTH * slab;
-    int* jbuf = reinterpret_cast<int*>(reinterpret_cast<double*>(tile_smem) +
-                                       static_cast<size_t>(kTileWarps) * DEPTH * slab) +
-                static_cast<size_t>(wid) * slab;
+    int* jbuf = JREG ? reinterpret_cast<int*>(wbuf + slab)
+                     : reinterpret_cast<int*>(reinterpret_cast<double*>(tile_smem) +
+                                              static_cast<size_t>(kTileWarps) * DEPTH * slab) +
+                           static_cast<size_t>(wid) * slab;
     const size_t N = static_cast<size_t>(n);
     const size_t nnz = N * static_cast<size_t>(k);
     const unsigned long long pol = evict_first_policy();
@@ -314,6 +318,15 @@ __global__ void __launch_bounds__(kTileWarps * 32) stream_collide_kernel(
                                 m, k, ks, lane, r0, c0, q32, r32, pol);
             cp_async_commit();
         }
+        int jrow[JREG ? KT : 1];
+        if constexpr (JREG) {  // the lane's index row, then the buffer is free
+            cp_async_wait<0>();
+            __syncwarp();
+            if (lane < cnt)
+#pragma unroll
+                for (int j = 0; j < KT; ++j) jrow[j] = jbuf[lane * ks + j];
+            __syncwarp();
+        }
         T f[9];
 #pragma unroll
         for (int a = 1; a < 9; ++a) {
@@ -330,11 +343,17 @@ __global__ void __launch_bounds__(kTileWarps * 32) stream_collide_kernel(
                 const double* wr = wbuf + ((a - 1) % DEPTH) * slab + lane * ks;
                 const int* jr = jbuf + lane * ks;
                 const T* pa = pdf_in + N * a;
-                T v = mul(static_cast<T>(wr[0]), pa[jr[0]]);
-                if constexpr (KT > 0) {
+                T v;
+                if constexpr (JREG) {
+                    v = mul(static_cast<T>(wr[0]), pa[jrow[0]]);
+#pragma unroll
+                    for (int j = 1; j < KT; ++j) v = fmaT(static_cast<T>(wr[j]), pa[jrow[j]], v);
+                } else if constexpr (KT > 0) {
+                    v = mul(static_cast<T>(wr[0]), pa[jr[0]]);
 #pragma unroll
                     for (int j = 1; j < KT; ++j) v = fmaT(static_cast<T>(wr[j]), pa[jr[j]], v);
                 } else {
+                    v = mul(static_cast<T>(wr[0]), pa[jr[0]]);
 #pragma unroll 8
                     for (int j = 1; j < k; ++j) v = fmaT(static_cast<T>(wr[j]), pa[jr[j]], v);
                 }
@@ -356,11 +375,11 @@ __global__ void __launch_bounds__(kTileWarps * 32) stream_collide_kernel(
     }
 }
 
-template <typename T, bool PAD, int KT, int DEPTH, bool VEC>
+template <typename T, bool PAD, int KT, int DEPTH, bool VEC, bool JREG = false>
 int launch_stream_collide(int n, int k, const int* ja, const double* W, T omega, const T* pin,
                           T* pout, T* rho, T* ux, T* uy, cudaStream_t st) {
-    auto kern = stream_collide_kernel<T, PAD, KT, DEPTH, VEC>;
-    const size_t smem = tile_smem_bytes(k, DEPTH);
+    auto kern = stream_collide_kernel<T, PAD, KT, DEPTH, VEC, JREG>;
+    const size_t smem = tile_smem_bytes(k, DEPTH, JREG);
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(smem)) != cudaSuccess)
         return RBFB_ECUDA;
@@ -383,16 +402,16 @@ int stream_collide(int n, int k, const int* ja, const double* W, T omega, const 
                    T* rho, T* ux, T* uy, cudaStream_t st) {
     // 16-byte copies need 16-byte aligned rows: ja, W and every direction's
     // array (n*k even). Odd k: unpadded slabs; k = 21 (the D2Q9 operators'
-    // usual stencil) fixed at compile time. Even k: padded slabs, 8-byte
-    // copies.
+    // usual stencil) fixed at compile time, with the index rows held in
+    // registers. Even k: padded slabs, 8-byte copies.
     const bool vec = ((reinterpret_cast<uintptr_t>(ja) | reinterpret_cast<uintptr_t>(W)) & 15) == 0 &&
                      ((static_cast<long long>(n) * k) & 1) == 0;
     if (!(k & 1))
         return launch_stream_collide<T, true, 0, 2, false>(n, k, ja, W, omega, pin, pout, rho, ux,
                                                            uy, st);
-    if (vec && k == 21)
-        return launch_stream_collide<T, false, 21, 2, true>(n, k, ja, W, omega, pin, pout, rho,
-                                                            ux, uy, st);
+    if (vec && k == 21)  // index rows in registers: no index slab, 20 warps per SM
+        return launch_stream_collide<T, false, 21, 2, true, true>(n, k, ja, W, omega, pin, pout,
+                                                                  rho, ux, uy, st);
     if (vec)
         return launch_stream_collide<T, false, 0, 2, true>(n, k, ja, W, omega, pin, pout, rho, ux,
                                                            uy, st);
