@@ -355,6 +355,9 @@ def config3(R, O, torch, ctx, dev, reps=3):
         del vals, info
     res["mixed_over_fp64"] = res["fp64"]["ms"] / res["mixed"]["ms"]
     res["error_sample"] = "2,048 stencils (64 boundary), FP64 CPU oracle"
+    res["launches_note"] = ("fp64: one assembly launch per call, after a device counting sort "
+                            "of the stencils by class (3 small kernels) and before the singular "
+                            "count; mixed: one launch per bucket plus its FP64 fallback launch")
     del w
     torch.cuda.synchronize()
     return res

@@ -2,9 +2,10 @@
 //
 // FP64 batches (up to 3 right-hand sides) run as ONE persistent launch of the
 // uneven kernel (asm_blocked.cuh, blk_csr_kernel): warps claim stencils of
-// any size and degree from a device counter; systems of up to 48 unknowns
-// are solved in shared memory, larger ones (up to 96) in an L2-resident
-// global scratch region per warp.
+// any size and degree from a device counter, walking a list sorted by class
+// on the device (largest systems first); systems of up to 48 unknowns are
+// solved in shared memory, larger ones (up to 96) in an L2-resident global
+// scratch region per warp.
 //
 // Other batches (the FP32-refinement form, more right-hand sides) are
 // bucketed on the device by the compiled kernel shape that fits them
@@ -32,10 +33,19 @@ namespace rbfb {
 namespace {
 
 // The single-launch FP64 kernel for uneven batches: systems of up to 48
-// unknowns in shared memory (three warps per CTA), up to 96 in global scratch.
-constexpr int kOneNS = 48, kOneNG = 96, kOneBlock = 32, kOnePB = 8;
+// unknowns in shared memory (one warp per CTA), up to 96 in global scratch.
+// Its n > 48 body (three list slots a lane) would set the register count
+// of every path (230); bounded to 11 CTAs per SM it fits in 168 registers,
+// spilling only on that rare path.
+constexpr int kOneNS = 48, kOneNG = 96, kOneBlock = 32, kOnePB = 8, kOneMinB = 11;
 using OneCfg = CsrCfg<double, kOneNS, kOneNG, 3, kOnePB>;
 constexpr int kOneSmem = OneCfg::SmemL::bytes * (kOneBlock / 32);
+// The launch walks the stencils sorted by class (system size descending,
+// then degree): warps on one SM then run the same fill and elimination
+// bodies (the instruction cache holds one at a time), and the largest
+// systems go first instead of forming the tail. kOneKeys classes.
+constexpr int kOneKeys = (kOneNG + 2) * 5;
+__host__ __device__ constexpr int one_key(int n, int P) { return (kOneNG + 1 - n) * 5 + P; }
 
 constexpr int kMaxVariants = 64;
 constexpr int kTabN = 161;  // system sizes 0..160
@@ -51,8 +61,10 @@ struct BatchState {
     size_t cap = 0;
     int* bucket_of = nullptr;
     int* list = nullptr;
-    // the single-launch kernel: persistent grid and its global scratch
+    // the single-launch kernel: persistent grid, its global scratch, and the
+    // class counts | offsets | cursors of its sorted stencil list
     int one_grid = 0;
+    int* one_counts = nullptr;
     char* gscratch = nullptr;
     size_t gscratch_bytes = 0;
     // cached graph of the last batch
@@ -88,6 +100,46 @@ __global__ void offsets_kernel(int* counts, int nb) {
         counts[kMaxVariants + b] = acc;   // offsets
         counts[2 * kMaxVariants + b] = 0; // cursors
         acc += counts[b];
+    }
+}
+
+// Class of every stencil of the single launch (an invalid one gets the
+// last class; the kernel flags it) and the class counts.
+__global__ void one_assign_kernel(int nst, const int* ia, const int8_t* degree, int P0,
+                                  int* key_of, int* counts) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nst; s += gridDim.x * blockDim.x) {
+        const int ks = ia[s + 1] - ia[s];
+        const int P = degree ? degree[s] : P0;
+        int key = kOneKeys - 1;
+        if (P >= 0 && P <= 4 && ks >= 1 && ks + npoly(P) <= kOneNG) key = one_key(ks + npoly(P), P);
+        key_of[s] = key;
+        atomicAdd(counts + key, 1);
+    }
+}
+
+__global__ void one_offsets_kernel(int* counts) {
+    __shared__ int part[kOneKeys];
+    for (int i = threadIdx.x; i < kOneKeys; i += blockDim.x) part[i] = counts[i];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int i = 0; i < kOneKeys; ++i) {
+            const int c = part[i];
+            part[i] = acc;
+            acc += c;
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kOneKeys; i += blockDim.x) {
+        counts[kOneKeys + i] = part[i];  // offsets
+        counts[2 * kOneKeys + i] = 0;    // cursors
+    }
+}
+
+__global__ void one_scatter_kernel(int nst, const int* key_of, int* counts, int* list) {
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < nst; s += gridDim.x * blockDim.x) {
+        const int key = key_of[s];
+        list[counts[kOneKeys + key] + atomicAdd(counts + 2 * kOneKeys + key, 1)] = s;
     }
 }
 
@@ -153,7 +205,8 @@ int build_table(rbfb_ctx* ctx, BatchState* b, bool mixed, int phs, int Pmin, int
 // stream capture).
 int ensure_one(rbfb_ctx* ctx, BatchState* b) {
     const void* k = reinterpret_cast<const void*>(
-        &blk_csr_kernel<double, kOneNS, kOneNG, 3, kOneBlock, kOnePB>);
+        &blk_csr_kernel<double, kOneNS, kOneNG, 3, kOneBlock, kOnePB, 0, kOneMinB>);
+    if (!b->one_counts) RBFB_CUDA(ctx, cudaMalloc(&b->one_counts, 3 * kOneKeys * sizeof(int)));
     if (b->one_grid == 0) {
         RBFB_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kOneSmem));
         int nb = 0;
@@ -174,6 +227,7 @@ int ensure_one(rbfb_ctx* ctx, BatchState* b) {
 
 void release(BatchState* b) {
     cudaFree(b->gscratch);
+    cudaFree(b->one_counts);
     cudaFree(b->table); cudaFree(b->counts); cudaFree(b->ctrs); cudaFree(b->err);
     cudaFree(b->bucket_of); cudaFree(b->list);
     if (b->graph) cudaGraphExecDestroy(b->graph);
@@ -268,15 +322,22 @@ int rbfb_assemble_csr(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const
         RBFB_CUDA(ctx, cudaMemsetAsync(b->ctrs, 0, kMaxVariants * sizeof(DevCounters), s));
         RBFB_CUDA(ctx, cudaMemsetAsync(b->err, 0, sizeof(int), s));
         if (nstencils == 0) return RBFB_OK;
+        // the stencils sorted by class (counting sort on the device)
+        RBFB_CUDA(ctx, cudaMemsetAsync(b->one_counts, 0, kOneKeys * sizeof(int), s));
+        const int blocks = std::max(1, std::min((nstencils + 255) / 256, ctx->sms * 8));
+        one_assign_kernel<<<blocks, 256, 0, s>>>(nstencils, ia, degree, desc->degree, b->bucket_of,
+                                                 b->one_counts);
+        one_offsets_kernel<<<1, 256, 0, s>>>(b->one_counts);
+        one_scatter_kernel<<<blocks, 256, 0, s>>>(nstencils, b->bucket_of, b->one_counts, b->list);
         AsmParams q = p;
-        q.list = nullptr;
+        q.list = b->list;
         q.item_base = 0;
         q.nitems = nstencils;
         q.work = &b->ctrs[0].work[0];
-        blk_csr_kernel<double, kOneNS, kOneNG, 3, kOneBlock, kOnePB>
+        blk_csr_kernel<double, kOneNS, kOneNG, 3, kOneBlock, kOnePB, 0, kOneMinB>
             <<<b->one_grid, kOneBlock, kOneSmem, s>>>(q, degree, desc->degree, desc->phs,
                                                        b->gscratch, b->err);
-        ctx->launches += 1;
+        ctx->launches += 4;
         RBFB_CUDA(ctx, cudaGetLastError());
         return RBFB_OK;
     };
@@ -325,7 +386,7 @@ int rbfb_assemble_csr(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const
             key.insert(key.end(), c, c + len);
         };
         const void* ptrs[] = {x, y, ia, ja, degree, info, b->list, b->bucket_of, b->counts,
-                              b->ctrs, ctx->fb_list, b->table, b->gscratch};
+                              b->ctrs, ctx->fb_list, b->table, b->gscratch, b->one_counts};
         put(ptrs, sizeof(ptrs));
         put(p.values, sizeof(p.values));
         put(&nstencils, sizeof(nstencils));
