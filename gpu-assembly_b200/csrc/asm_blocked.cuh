@@ -1003,21 +1003,17 @@ __device__ __forceinline__ void assemble_any(const AsmParams& p, int s, int off,
     scatter_regs<T, L::R, NRHS, G>(p, xs, np, ks, off, e, info, s, lane);
 }
 
-template <typename T, int NS, int NG, int NRHS, int PB, int NSMALL = 0>
+template <typename T, int NS, int NG, int NRHS, int PB>
 struct CsrCfg {
     using SmemL = BlkLayout<T, NS, NRHS, NS, PB, 32, false>;  // shared-memory slot
     using GlobL = BlkLayout<T, NG, NRHS, NG, PB, 32, false>;  // global scratch region
-    // systems of up to NSMALL unknowns: one list slot a lane, in the same slot
-    using SmallL = BlkLayout<T, (NSMALL > 0 ? NSMALL : 32), NRHS, (NSMALL > 0 ? NSMALL : 32), PB,
-                             32, false>;
-    static_assert(SmallL::bytes <= SmemL::bytes, "the small layout fits the slot");
     static constexpr size_t gbytes = (static_cast<size_t>(GlobL::bytes) + 255) & ~size_t(255);
 };
 
-template <typename T, int NS, int NG, int NRHS, int BLOCK, int PB, int NSMALL = 0, int MINB = 1>
+template <typename T, int NS, int NG, int NRHS, int BLOCK, int PB, int MINB = 1>
 __global__ void __launch_bounds__(BLOCK, MINB)
     blk_csr_kernel(AsmParams p, const int8_t* degree, int P0, int phs, char* gscratch, int* err) {
-    using C = CsrCfg<T, NS, NG, NRHS, PB, NSMALL>;
+    using C = CsrCfg<T, NS, NG, NRHS, PB>;
     constexpr int G = 32, GPB = BLOCK / G;
     extern __shared__ __align__(16) char smem_raw[];
     const int gib = threadIdx.x / 32;
@@ -1042,9 +1038,7 @@ __global__ void __launch_bounds__(BLOCK, MINB)
             if (lane == 0) atomicExch(err, 1);
             continue;
         }
-        if (NSMALL > 0 && n <= NSMALL)
-            assemble_any<T, typename C::SmallL, NRHS, PB>(p, s, off, ks, P, Q, slot, lane);
-        else if (n <= NS)
+        if (n <= NS)
             assemble_any<T, typename C::SmemL, NRHS, PB>(p, s, off, ks, P, Q, slot, lane);
         else
             assemble_any<T, typename C::GlobL, NRHS, PB>(p, s, off, ks, P, Q, gslot, lane);

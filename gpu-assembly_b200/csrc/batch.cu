@@ -205,7 +205,7 @@ int build_table(rbfb_ctx* ctx, BatchState* b, bool mixed, int phs, int Pmin, int
 // stream capture).
 int ensure_one(rbfb_ctx* ctx, BatchState* b) {
     const void* k = reinterpret_cast<const void*>(
-        &blk_csr_kernel<double, kOneNS, kOneNG, 3, kOneBlock, kOnePB, 0, kOneMinB>);
+        &blk_csr_kernel<double, kOneNS, kOneNG, 3, kOneBlock, kOnePB, kOneMinB>);
     if (!b->one_counts) RBFB_CUDA(ctx, cudaMalloc(&b->one_counts, 3 * kOneKeys * sizeof(int)));
     if (b->one_grid == 0) {
         RBFB_CUDA(ctx, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kOneSmem));
@@ -334,7 +334,7 @@ int rbfb_assemble_csr(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const
         q.item_base = 0;
         q.nitems = nstencils;
         q.work = &b->ctrs[0].work[0];
-        blk_csr_kernel<double, kOneNS, kOneNG, 3, kOneBlock, kOnePB, 0, kOneMinB>
+        blk_csr_kernel<double, kOneNS, kOneNG, 3, kOneBlock, kOnePB, kOneMinB>
             <<<b->one_grid, kOneBlock, kOneSmem, s>>>(q, degree, desc->degree, desc->phs,
                                                        b->gscratch, b->err);
         ctx->launches += 4;
