@@ -194,11 +194,15 @@ int rbfb_assemble_range(rbfb_ctx* ctx, const rbfb_desc* desc, int first, int cou
                         void* stream);
 
 /* Ragged stencils in CSR form (ia has nstencils+1 entries), optionally with a
- * per-stencil degree (int8, NULL = desc->degree): the uneven batch. Stencils
- * are bucketed on the device by system size and each bucket runs as one
- * persistent launch of the kernel shape that fits it. The call is a fixed
- * launch sequence with no host round trip; on a non-default stream it is
- * captured in a CUDA graph and replayed when the same batch comes again.
+ * per-stencil degree (int8, NULL = desc->degree): the uneven batch. FP64
+ * with up to 3 right-hand sides: the whole batch in ONE persistent launch,
+ * its warps taking the stencils in class order (system size descending,
+ * then degree) from a list sorted on the device; systems of up to 96
+ * unknowns. The refined form (and more right-hand sides): stencils bucketed
+ * on the device by system size, one persistent launch per bucket of the
+ * kernel shape that fits it. The call is a fixed launch sequence with no
+ * host round trip; on a non-default stream it is captured in a CUDA graph
+ * and replayed when the same batch comes again.
  * The Fortran module's fill_kernel (src/rbf_cuda.f90:36-99) is the
  * reference's only CSR-driven assembly. */
 int rbfb_assemble_csr(rbfb_ctx* ctx, const rbfb_desc* desc, int nstencils, const double* x,
