@@ -202,6 +202,16 @@ def test_spmv_with_boundary_fix(ctx, torch_cuda):
     T.cuda.synchronize()
     ref = O.spmv(g["ja_nanoflann"], W[0], u, k, bnd)
     np.testing.assert_array_equal(out.cpu().numpy(), ref)  # same order, bit for bit
+    # weights and columns off a 16-byte boundary: scalar loads, the same sums
+    Wb = T.empty(W[0].size + 1, dtype=T.float64, device="cuda")
+    jb = T.empty(n * k + 1, dtype=T.int32, device="cuda")
+    Wu, ju = Wb[1:], jb[1:]
+    Wu.copy_(Wd)
+    ju.copy_(jad)
+    out2 = T.empty_like(out)
+    R.spmv(n, k, ju, Wu, ud, out2, bd)
+    T.cuda.synchronize()
+    np.testing.assert_array_equal(out2.cpu().numpy(), ref)
     # and it is a Laplacian: -13 u in the interior up to the discretisation error
     interior = np.setdiff1d(np.arange(n), bnd)
     assert np.abs(ref[interior] + 13 * u[interior]).max() < 0.5

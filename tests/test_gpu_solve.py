@@ -53,6 +53,29 @@ def test_solve_bit_identical(ctx, torch_cuda, n, nb, use_stream):
     assert np.abs(u - u_exact(pr["x"], pr["y"])).max() < 2e-3
 
 
+def test_solve_unaligned_operator_arrays(ctx, torch_cuda):
+    """Weights and columns that start off a 16-byte boundary: the operator
+    passes then walk the rows with scalar loads instead of staging them with
+    16-byte copies. The iterate is the same, bit for bit."""
+    T = torch_cuda
+    pr = poisson_disk(n=2000, nb=160)
+    L, ja, f, n = pr["L"], pr["ja"], pr["f"], pr["n"]
+    Lb = T.empty(L.size + 1, dtype=T.float64, device="cuda")
+    jb = T.empty(ja.size + 1, dtype=T.int32, device="cuda")
+    Ld, jd = Lb[1:], jb[1:]  # 8 and 4 bytes past the allocation's start
+    assert Ld.data_ptr() % 16 and jd.data_ptr() % 16
+    Ld.copy_(T.as_tensor(L))
+    jd.copy_(T.as_tensor(ja))
+    ud = T.zeros(n, dtype=T.float64, device="cuda")
+    st, it, rel = ctx.solve_bicgstab(Ld, jd, _dev(T, f), ud, k=pr["k"], bnd=_dev(T, pr["bnd"]),
+                                     tol=1e-12, maxit=20000)
+    ost, ou, oit, orel = O.bicgstab(L, ja, f, np.zeros(n), k=pr["k"], bnd=pr["bnd"], tol=1e-12,
+                                    maxit=20000, grid=O.solve_grid(n, _sms(T)))
+    assert st == R.OK and ost == 0
+    assert it == oit and rel == orel
+    np.testing.assert_array_equal(ud.cpu().numpy(), ou)
+
+
 def test_solve_graph_replay_and_launches(ctx, torch_cuda):
     # a non-default stream captures one chunk of 8 iterations (5 kernels
     # each) once and replays it
