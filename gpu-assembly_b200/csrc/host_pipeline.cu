@@ -1,10 +1,13 @@
 // host_pipeline.cu -- rbfb_assemble_host: the end-to-end call from host
-// memory. Nodes go in once; the k-NN search and the assembly run on a
-// compute stream in chunks of stencils, and each chunk's weights are copied
-// back on a second stream as soon as the chunk is done, so the device->host
-// transfer of the CSR values (the largest transfer of the call) overlaps the
-// assembly of the next chunks. Copies are asynchronous, and overlap, when the
-// host buffers are pinned (cudaHostAlloc / cudaHostRegister).
+// memory. Nodes go in once; the k-NN search runs on a compute stream, then
+// the assembly in chunks of stencils, alternating between two compute
+// streams so that a chunk's kernel fills the SMs its predecessor's last
+// CTAs leave idle (the chunks' outputs are disjoint and their kernels
+// assign stencils statically). Each chunk's weights are copied back on a
+// third stream as soon as the chunk is done, so the device->host transfer
+// of the CSR values (the largest transfer of the call) overlaps the
+// assembly of the next chunks. Copies are asynchronous, and overlap, when
+// the host buffers are pinned (cudaHostAlloc / cudaHostRegister).
 //
 // No reference counterpart: the reference's caller copies and launches by
 // hand (src/main.cpp:27-53, src/main.f90:25-57).
@@ -29,7 +32,7 @@ struct Pipe {
     int* fb = nullptr;
     double* vals[kMaxRhs] = {};
     DevCounters* ctrs = nullptr;
-    cudaStream_t sc = nullptr, sd = nullptr;
+    cudaStream_t sc = nullptr, sc2 = nullptr, sd = nullptr;
     std::vector<cudaEvent_t> ev;
     cudaEvent_t t0 = nullptr, t1 = nullptr, kdone = nullptr;
 };
@@ -42,6 +45,7 @@ Pipe* pipe_of(rbfb_ctx* ctx) {
 int grow(rbfb_ctx* ctx, Pipe* p, size_t n, size_t nk, int nrhs, int nchunk) {
     if (!p->sc) {
         RBFB_CUDA(ctx, cudaStreamCreateWithFlags(&p->sc, cudaStreamNonBlocking));
+        RBFB_CUDA(ctx, cudaStreamCreateWithFlags(&p->sc2, cudaStreamNonBlocking));
         RBFB_CUDA(ctx, cudaStreamCreateWithFlags(&p->sd, cudaStreamNonBlocking));
         RBFB_CUDA(ctx, cudaEventCreate(&p->t0));
         RBFB_CUDA(ctx, cudaEventCreate(&p->t1));
@@ -97,6 +101,7 @@ void rbfb_release_pipeline(rbfb_ctx* ctx) {
     if (p->t1) cudaEventDestroy(p->t1);
     if (p->kdone) cudaEventDestroy(p->kdone);
     if (p->sc) cudaStreamDestroy(p->sc);
+    if (p->sc2) cudaStreamDestroy(p->sc2);
     if (p->sd) cudaStreamDestroy(p->sd);
     delete p;
     ctx->pipe = nullptr;
@@ -119,12 +124,12 @@ int rbfb_assemble_host(rbfb_ctx* ctx, const rbfb_desc* desc, int n, const double
         if (!values_h[q]) return fail(ctx, RBFB_EINVAL, "null host values pointer");
     RBFB_CUDA(ctx, cudaSetDevice(ctx->device));
     const size_t nk = static_cast<size_t>(n) * k;
-    const int chunk = std::max(32768, (n + 15) / 16);
+    const int chunk = std::max(16384, (n + 63) / 64);
     const int nchunk = (n + chunk - 1) / chunk;
     Pipe* p = pipe_of(ctx);
     rc = grow(ctx, p, n, nk, nrhs, nchunk);
     if (rc) return rc;
-    cudaStream_t sc = p->sc, sd = p->sd;
+    cudaStream_t sc = p->sc, sc2 = p->sc2, sd = p->sd;
     RBFB_CUDA(ctx, cudaEventRecord(p->t0, sc));
     RBFB_CUDA(ctx, cudaMemcpyAsync(p->x, x_h, n * sizeof(double), cudaMemcpyHostToDevice, sc));
     RBFB_CUDA(ctx, cudaMemcpyAsync(p->y, y_h, n * sizeof(double), cudaMemcpyHostToDevice, sc));
@@ -144,12 +149,16 @@ int rbfb_assemble_host(rbfb_ctx* ctx, const rbfb_desc* desc, int n, const double
         RBFB_CUDA(ctx, cudaMemcpyAsync(ja_out_h, p->ja, nk * sizeof(int), cudaMemcpyDeviceToHost, sd));
     }
     RBFB_CUDA(ctx, cudaMemsetAsync(p->ctrs, 0, nchunk * sizeof(DevCounters), sc));
+    // the second compute stream starts after the stencils and counters
+    RBFB_CUDA(ctx, cudaEventRecord(p->kdone, sc));
+    RBFB_CUDA(ctx, cudaStreamWaitEvent(sc2, p->kdone, 0));
     for (int c = 0; c < nchunk; ++c) {
         const int c0 = c * chunk, cnt = std::min(chunk, n - c0);
+        cudaStream_t s = (c & 1) ? sc2 : sc;
         rc = enqueue_fixed(ctx, desc, c0, cnt, p->x, p->y, k, p->ja, p->vals, p->info,
-                           p->ctrs + c, p->fb + c0, sc);
+                           p->ctrs + c, p->fb + c0, s);
         if (rc) return rc;
-        RBFB_CUDA(ctx, cudaEventRecord(p->ev[c], sc));
+        RBFB_CUDA(ctx, cudaEventRecord(p->ev[c], s));
         RBFB_CUDA(ctx, cudaStreamWaitEvent(sd, p->ev[c], 0));
         const size_t o = static_cast<size_t>(c0) * k, len = static_cast<size_t>(cnt) * k;
         for (int q = 0; q < nrhs; ++q)
@@ -159,7 +168,10 @@ int rbfb_assemble_host(rbfb_ctx* ctx, const rbfb_desc* desc, int n, const double
             RBFB_CUDA(ctx, cudaMemcpyAsync(info_h + c0, p->info + c0, cnt * sizeof(int),
                                            cudaMemcpyDeviceToHost, sd));
     }
-    // singular count on the device, then the counters of every chunk
+    // both compute streams done: singular count on the device, then the
+    // counters of every chunk
+    RBFB_CUDA(ctx, cudaEventRecord(p->kdone, sc2));
+    RBFB_CUDA(ctx, cudaStreamWaitEvent(sc, p->kdone, 0));
     rc = count_singular(ctx, p->info, n, &p->ctrs[0].singular, sc);
     if (rc) return rc;
     std::vector<DevCounters> h(nchunk);
