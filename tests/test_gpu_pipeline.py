@@ -86,6 +86,41 @@ def test_csr_uneven_matches_oracle(ctx, torch_cuda):
         assert worst <= tol, (prec, worst)
 
 
+def test_csr_unsupported_stencil_is_reported(ctx, torch_cuda):
+    """One stencil of an unsupported degree in an FP64 uneven batch: the
+    one launch skips it (it sorts into the last class) and the call reports
+    EUNSUPPORTED; every other stencil is assembled, bit-identical to the
+    oracle."""
+    T = torch_cuda
+    c = NS.config_disk_uneven(n=3000, nb=120, seed=19)
+    kvec, x, y = c["kvec"], c["x"], c["y"]
+    n = x.size
+    kmax = int(kvec.max())
+    jaf = O.knn_brute(x, y, kmax).reshape(n, kmax)
+    ia = np.zeros(n + 1, np.int32)
+    ia[1:] = np.cumsum(kvec)
+    ja = np.concatenate([jaf[s, : kvec[s]] for s in range(n)]).astype(np.int32)
+    deg = c["degree"].copy()
+    bad = 7
+    deg[bad] = 5  # no kernel takes degree 5
+    vals = [T.full((int(ia[-1]),), float("nan"), dtype=T.float64, device="cuda") for _ in range(3)]
+    info = T.full((n,), -3, dtype=T.int32, device="cuda")
+    with pytest.raises(R.RbfError) as e:
+        ctx.assemble_csr(R.make_desc(2), T.as_tensor(x).cuda(), T.as_tensor(y).cuda(),
+                         T.as_tensor(ia).cuda(), T.as_tensor(ja).cuda(), vals,
+                         degree=T.as_tensor(deg).cuda(), info=info, stats=True)
+    assert e.value.status == R.EUNSUPPORTED
+    T.cuda.synchronize()
+    W = np.stack([v.cpu().numpy() for v in vals])
+    Wo, _ = O.assemble_csr(x, y, ia, ja, degree=c["degree"], P=2, Q=0)
+    keep = np.ones(int(ia[-1]), bool)
+    keep[ia[bad]:ia[bad + 1]] = False
+    np.testing.assert_array_equal(W[:, keep], Wo[:, keep])
+    assert np.isnan(W[:, ~keep]).all()  # the skipped stencil's row is untouched
+    io = info.cpu().numpy()
+    assert io[bad] == -3 and (np.delete(io, bad) == 0).all()
+
+
 def test_autotune_picks_a_compiled_shape(ctx, torch_cuda):
     T = torch_cuda
     g = golden("square69_k21")
