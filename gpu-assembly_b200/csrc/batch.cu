@@ -3,7 +3,7 @@
 // FP64 batches (up to 3 right-hand sides) run as ONE persistent launch of the
 // uneven kernel (asm_blocked.cuh, blk_csr_kernel): warps claim stencils of
 // any size and degree from a device counter, walking a list sorted by class
-// on the device (largest systems first); systems of up to 48 unknowns are
+// on the device (largest systems first); systems of up to 45 unknowns are
 // solved in shared memory, larger ones (up to 96) in an L2-resident global
 // scratch region per warp.
 //
@@ -32,12 +32,13 @@
 namespace rbfb {
 namespace {
 
-// The single-launch FP64 kernel for uneven batches: systems of up to 48
-// unknowns in shared memory (one warp per CTA), up to 96 in global scratch.
-// Its n > 48 body (three list slots a lane) would set the register count
-// of every path (230); bounded to 11 CTAs per SM it fits in 168 registers,
-// spilling only on that rare path.
-constexpr int kOneNS = 48, kOneNG = 96, kOneBlock = 32, kOnePB = 8, kOneMinB = 11;
+// The single-launch FP64 kernel for uneven batches: systems of up to 45
+// unknowns (degree 3 with k = 35, the largest interior stencil in common
+// use) in a 19 KB shared-memory slot, 11 CTAs of one warp per SM; up to 96
+// in global scratch. Its n > 45 body (three list slots a lane) would set
+// the register count of every path (230); bounded to 11 CTAs per SM it fits
+// in 168 registers, spilling only on that rare path.
+constexpr int kOneNS = 45, kOneNG = 96, kOneBlock = 32, kOnePB = 8, kOneMinB = 11;
 using OneCfg = CsrCfg<double, kOneNS, kOneNG, 3, kOnePB>;
 constexpr int kOneSmem = OneCfg::SmemL::bytes * (kOneBlock / 32);
 // The launch walks the stencils sorted by class (system size descending,
